@@ -1,0 +1,128 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes front end of the CPU checker (librh_oracle.so).
+
+The checker restates RAMSES II's FP64 CPU hydro step (hydro/umuscl.f90,
+hydro/godunov_utils.f90, hydro/godunov_fine.f90, hydro/courant_fine.f90).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs use it.
+Parity status: unpinned against the reference binary (no Fortran compiler in
+the image, no golden vectors shipped by the reference); pinned by the
+known-answer tests in tests/.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from ramses2_b200._abi import HydroParams, MeshDesc, dptr
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librh_oracle.so")
+_lib = None
+
+
+def build():
+    """Compile librh_oracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        L.rh_oracle_riemann.argtypes = [C.c_int, P(C.c_double), P(C.c_double), P(HydroParams),
+                                        C.c_double, P(C.c_double)]
+        L.rh_oracle_unsplit.argtypes = [C.c_int, P(C.c_double), C.c_double, C.c_double,
+                                        P(HydroParams), P(C.c_double)]
+        L.rh_oracle_cmpdt.argtypes = [P(C.c_double), P(C.c_double), C.c_double, P(HydroParams), C.c_int]
+        L.rh_oracle_cmpdt.restype = C.c_double
+        L.rh_oracle_interpol_hydro.argtypes = [P(C.c_double), P(C.c_double), C.c_int, C.c_int, C.c_double]
+        L.rh_oracle_godunov_fine.argtypes = [P(MeshDesc), P(HydroParams), C.c_int, C.c_double,
+                                             P(C.c_double), P(C.c_double), C.c_int]
+        L.rh_oracle_courant_fine.argtypes = [P(MeshDesc), P(HydroParams), C.c_int, P(C.c_double),
+                                             P(C.c_double)]
+        L.rh_oracle_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise RuntimeError("oracle error %d: %s" % (rc, lib().rh_oracle_last_error().decode()))
+
+
+def riemann(solver, ql, qr, params, smax_cap=np.finfo(np.float64).max):
+    ql = np.ascontiguousarray(ql, np.float64)
+    qr = np.ascontiguousarray(qr, np.float64)
+    out = np.zeros(6)
+    _check(lib().rh_oracle_riemann(solver, dptr(ql), dptr(qr), C.byref(params), smax_cap, dptr(out)))
+    return out
+
+
+def unsplit(uin, dx, dt, params):
+    """uin: (5, nn+4, nn+4, nn+4) indexed [var, k, j, i] -> flux (3, 5, nn+1, nn+1, nn+1)."""
+    nn = uin.shape[-1] - 4
+    u = np.ascontiguousarray(uin, np.float64)
+    out = np.zeros((3, 5, nn + 1, nn + 1, nn + 1))
+    _check(lib().rh_oracle_unsplit(nn, dptr(u), dx, dt, C.byref(params), dptr(out)))
+    return out
+
+
+def cmpdt(uu, dx, params, grav=(0.0, 0.0, 0.0), ndim=3):
+    uu = np.ascontiguousarray(uu, np.float64)
+    g = np.ascontiguousarray(grav, np.float64)
+    return lib().rh_oracle_cmpdt(dptr(uu), dptr(g), dx, C.byref(params), ndim)
+
+
+def interpol_hydro(u1, interpol_var, interpol_type, smallr=1e-10):
+    """u1: (5, 7) [var, j] -> u2 (5, 8) [var, ind]."""
+    a = np.ascontiguousarray(u1, np.float64)
+    out = np.zeros((5, 8))
+    _check(lib().rh_oracle_interpol_hydro(dptr(a), dptr(out), interpol_var, interpol_type, smallr))
+    return out
+
+
+class OracleHydro:
+    """The reference's per-level leaf calls, restated on the CPU.
+
+    Mirrors r_courant_fine / r_set_unew / r_godunov_fine / r_set_uold
+    (hydro/courant_fine.f90:18-52, hydro/godunov_fine.f90:13-214) on a
+    :class:`ramses2_b200.mesh.Mesh`.
+    """
+
+    def __init__(self, mesh, params, nthreads=1):
+        self.mesh = mesh
+        self.params = params
+        self.nthreads = nthreads
+        self.unew = mesh.uold.copy()
+
+    def courant_fine(self, ilevel):
+        out = np.zeros(5)
+        _check(lib().rh_oracle_courant_fine(C.byref(self.mesh.desc()), C.byref(self.params), ilevel,
+                                            dptr(self.mesh.uold), dptr(out)))
+        return out  # mass, ekin, eint, emag, dt
+
+    def set_unew(self, ilevel):
+        sl = self.mesh.level_slice(ilevel)
+        self.unew[sl] = self.mesh.uold[sl]
+
+    def set_uold(self, ilevel):
+        sl = self.mesh.level_slice(ilevel)
+        self.mesh.uold[sl] = self.unew[sl]
+
+    def godunov_fine(self, ilevel, dt):
+        _check(lib().rh_oracle_godunov_fine(C.byref(self.mesh.desc()), C.byref(self.params), ilevel,
+                                            dt, dptr(self.mesh.uold), dptr(self.unew), self.nthreads))
+
+    def step_uniform(self, dt=None):
+        """One coarse step of a single-level run (amr/amr_step.f90:276-455 order)."""
+        lev = self.mesh.levelmin
+        out = self.courant_fine(lev)
+        dx = self.mesh.dx(lev)
+        dtnew = min(dx / self.params.smallc, out[4]) if dt is None else dt
+        self.set_unew(lev)
+        self.godunov_fine(lev, dtnew)
+        self.set_uold(lev)
+        return dtnew, out

@@ -1,0 +1,69 @@
+/*
+ * rh_oracle.h — TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement (FP64, loop-faithful) of RAMSES II's unsplit MUSCL-Hancock
+ * Godunov hydro step, used as the checker for the CUDA path.  Only tests/,
+ * __graft_entry__.smoke() and bench.py's cpu_baseline / reference legs may
+ * load this library; the product path never links or calls it.
+ *
+ * Parity status: UNPINNED against the reference binary.  The reference path is
+ * Fortran / CUDA Fortran and no Fortran compiler exists in the build image, and
+ * the reference ships no golden vectors for this path.  The restatement is
+ * pinned instead by known-answer physics (analytic Sedov solution generated
+ * from the reference's own utils/py/sedov.py, exact conservation, symmetry,
+ * translation/rotation invariance) — see tests/.
+ *
+ * Every function cites the reference file:line it restates.
+ */
+#ifndef RH_ORACLE_H
+#define RH_ORACLE_H
+
+#include <stdint.h>
+#include "../include/ramses_hydro.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One HLLC/HLL/LLF interface solve: qleft/qright = (rho, un, ut1, ut2, p),
+ * fgdnv[0..5] = (mass, normal mom, t1 mom, t2 mom, energy, internal-energy).
+ * godunov_utils.f90:338-852 */
+int rh_oracle_riemann(int solver, const double* qleft, const double* qright,
+                      const rh_hydro_params* p, double smax_cap, double* fgdnv);
+
+/* unsplit() on one gathered stencil (umuscl.f90:20-292).
+ * nn = 2*nsubgrid cells per tile edge; uin is Fortran-ordered
+ * uin(-1:nn+2,-1:nn+2,-1:nn+2,1:5); flux_out is flux(1:nn+1,1:nn+1,1:nn+1,1:5,1:3)
+ * holding fx*dt/dx (entries outside the ranges unsplit writes are left 0). */
+int rh_oracle_unsplit(int nn, const double* uin, double dx, double dt,
+                      const rh_hydro_params* p, double* flux_out);
+
+/* cmpdt() for one cell (godunov_utils.f90:228-333); uu = conserved (5). */
+double rh_oracle_cmpdt(const double* uu, const double* grav, double dx,
+                       const rh_hydro_params* p, int ndim);
+
+/* interpol_hydro() (interpol_hydro.f90:5-109): u1(0:6,1:5) -> u2(1:8,1:5),
+ * both Fortran-ordered (first index fastest). */
+int rh_oracle_interpol_hydro(const double* u1, double* u2, int interpol_var,
+                             int interpol_type, double smallr);
+
+/* godunov_fine() for one level (godunov_fine.f90:43-79 + godfine1 244-1342).
+ * uold/unew are Fortran-ordered uold(1:8,1:5,1:ngrid) with oct igrid stored at
+ * offset (igrid-1)*40.  unew must already hold set_unew's copy (and any
+ * coarse-update contributions of finer levels).  nthreads>1 parallelises over
+ * oct blocks when no coarse update is needed (ilevel==levelmin). */
+int rh_oracle_godunov_fine(const rh_mesh_desc* m, const rh_hydro_params* p,
+                           int ilevel, double dt, const double* uold,
+                           double* unew, int nthreads);
+
+/* courant_fine() for one level (courant_fine.f90:57-168).
+ * out = (mass, ekin, eint, emag, dt). */
+int rh_oracle_courant_fine(const rh_mesh_desc* m, const rh_hydro_params* p,
+                           int ilevel, const double* uold, double* out);
+
+const char* rh_oracle_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

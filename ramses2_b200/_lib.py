@@ -1,0 +1,71 @@
+"""Loader of librh_b200.so, the in-tree sm_100a CUDA library.
+
+There is no CPU fallback: if the library is missing or cannot be loaded, every
+entry point of this package raises.
+"""
+import ctypes as C
+import os
+
+from ._abi import HydroParams, MeshDesc, STATUS
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librh_b200.so")
+
+_lib = None
+
+# name -> (restype, argtypes); mirrors include/ramses_hydro.h and the
+# extension entry points declared in include/ramses_hydro_ext.h
+_P = C.POINTER
+_d = C.c_double
+_i = C.c_int
+SIGNATURES = {
+    "rh_init": (_i, [_i]),
+    "rh_finalize": (_i, []),
+    "rh_last_error": (C.c_char_p, []),
+    "rh_sync": (_i, []),
+    "rh_set_precision": (_i, [_i]),
+    "rh_set_mesh": (_i, [_P(MeshDesc), _P(_d), _i, _i]),
+    "rh_set_grid_device": (_i, [_P(_d), _i, _i, _i]),
+    "rh_transfer_grid_host": (_i, [_P(_d), _i, _i, _i]),
+    "rh_set_unew": (_i, [_i, _i]),
+    "rh_set_uold": (_i, [_i, _i]),
+    "rh_cmpdt": (_i, [_i, _i, _d, _d, _d, _d, _d, _P(_d), _P(_d), _P(_d), _P(_d), _P(_d), _P(_d)]),
+    "rh_godunov": (_i, [_i, _i, _i, _i, _i, _i, _d, _d, _d, _d, _d, _d, _i, _i, _P(_d)]),
+    "rh_set_interpolation": (_i, [_i, _i]),
+    # extensions (include/ramses_hydro_ext.h)
+    "rh_set_tile": (_i, [_i, _i, _i]),
+    "rh_get_tile": (_i, [_P(_i), _P(_i), _P(_i)]),
+    "rh_list_tiles": (_i, [_i, _P(_i), _P(_i), _i]),
+    "rh_level_info": (_i, [_i, _P(_i), _P(C.c_longlong)]),
+    "rh_state_ptrs": (_i, [_P(C.c_void_p), _P(C.c_void_p), _P(C.c_void_p), _P(C.c_void_p)]),
+    "rh_bench_godunov": (_i, [_i, _i, _d, _d, _d, _d, _d, _d, _i, _i, _P(C.c_float)]),
+}
+
+
+class RHError(RuntimeError):
+    pass
+
+
+def lib():
+    """Load (and type) librh_b200.so; raise if it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RHError("librh_b200.so is not built: run `python -m ramses2_b200.build` "
+                          "(or __graft_entry__.build()); there is no CPU fallback")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name, None)
+            if f is None:
+                continue
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc, what=""):
+    if rc != 0:
+        msg = lib().rh_last_error().decode()
+        raise RHError("%s failed: %s (%s)" % (what or "rh call", STATUS.get(rc, rc), msg))
+    return rc

@@ -1,0 +1,911 @@
+// rh_api.cu — the C ABI of include/ramses_hydro.h: device state, pencil-table
+// builder, the four hydro leaf calls and their auxiliary kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "rh_internal.h"
+#include "rh_launch.h"
+
+namespace rh {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  set_error("%s: %s", what, cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? RH_ENOMEM : RH_ECUDA;
+}
+
+Context& ctx() {
+  static Context c;
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// kernel registry
+// ---------------------------------------------------------------------------
+struct RegEntry {
+  KernelKey k;
+  LaunchFn fn;
+  size_t smem;
+  int threads;
+};
+static std::vector<RegEntry>& registry() {
+  static std::vector<RegEntry> r;
+  return r;
+}
+void register_launcher(const KernelKey& k, LaunchFn fn, size_t smem, int threads) {
+  registry().push_back({k, fn, smem, threads});
+}
+LaunchFn find_launcher(int prec, int txo, int tyo, int slope, int riemann, size_t* smem, int* threads) {
+  for (auto& e : registry())
+    if (e.k.prec == prec && e.k.txo == txo && e.k.tyo == tyo && e.k.slope == slope && e.k.riemann == riemann) {
+      if (smem) *smem = e.smem;
+      if (threads) *threads = e.threads;
+      return e.fn;
+    }
+  return nullptr;
+}
+int list_tiles(int prec, int* txo, int* tyo, int max) {
+  int n = 0;
+  for (auto& e : registry()) {
+    if (e.k.prec != prec || e.k.slope != 2 || e.k.riemann != 3) continue;
+    if (n < max) { txo[n] = e.k.txo; tyo[n] = e.k.tyo; }
+    ++n;
+  }
+  return n;
+}
+
+// ---------------------------------------------------------------------------
+// auxiliary kernels
+// ---------------------------------------------------------------------------
+// FP32-bulk packing: [oct][5][8] double -> [oct][4][8] float + [oct][8] double
+__global__ void pack_bulk_kernel(const double* __restrict__ src, float* __restrict__ uf, double* __restrict__ ue,
+                                 long long noct) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= noct * 40) return;
+  long long oct = i / 40;
+  int r = (int)(i % 40), var = r / 8, cell = r % 8;
+  if (var < 4) uf[oct * 32 + var * 8 + cell] = (float)src[i];
+  else ue[oct * 8 + cell] = src[i];
+}
+__global__ void unpack_bulk_kernel(double* __restrict__ dst, const float* __restrict__ uf,
+                                   const double* __restrict__ ue, long long noct) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= noct * 40) return;
+  long long oct = i / 40;
+  int r = (int)(i % 40), var = r / 8, cell = r % 8;
+  dst[i] = var < 4 ? (double)uf[oct * 32 + var * 8 + cell] : ue[oct * 8 + cell];
+}
+template <typename E> __global__ void copy_kernel(E* __restrict__ dst, const E* __restrict__ src, long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long stride = (long long)gridDim.x * blockDim.x;
+  for (; i < n; i += stride) dst[i] = src[i];
+}
+
+// courant_fine over the leaf cells of [oct0, oct0+noct) of uold:
+// per-block partial (mass, ekin, eint, emag, dt).  hydro/courant_fine.f90:57-168
+__global__ void cmpdt_kernel(const double* __restrict__ ud, const float* __restrict__ uf, int fp32,
+                             const uint8_t* __restrict__ refined, long long oct0, long long noct, CflConst C,
+                             double vol, double* __restrict__ partial) {
+  __shared__ double red[32][4];
+  long long cell_id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double m = 0, ek = 0, ei = 0, dt = 1e300;
+  if (cell_id < noct * 8) {
+    long long oct = oct0 + cell_id / 8;
+    int cell = (int)(cell_id % 8);
+    if (!refined || !refined[cell_id]) {
+      double r, m1, m2, m3, E;
+      if (!fp32) {
+        const double* o = ud + oct * 40 + cell;
+        r = o[0]; m1 = o[8]; m2 = o[16]; m3 = o[24]; E = o[32];
+      } else {
+        const float* o = uf + oct * 32 + cell;
+        r = o[0]; m1 = o[8]; m2 = o[16]; m3 = o[24]; E = ud[oct * 8 + cell];
+      }
+      m = r * vol;
+      ek = E * vol;
+      const double rm = r > C.smallr ? r : C.smallr;
+      ei = E * vol;
+      ei -= 0.5 * (m1 * m1) / rm * vol;
+      ei -= 0.5 * (m2 * m2) / rm * vol;
+      ei -= 0.5 * (m3 * m3) / rm * vol;
+      dt = cmpdt_cell(r, m1, m2, m3, E, C);
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    m += __shfl_down_sync(0xffffffffu, m, off);
+    ek += __shfl_down_sync(0xffffffffu, ek, off);
+    ei += __shfl_down_sync(0xffffffffu, ei, off);
+    double o = __shfl_down_sync(0xffffffffu, dt, off);
+    dt = o < dt ? o : dt;
+  }
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { red[w][0] = m; red[w][1] = ek; red[w][2] = ei; red[w][3] = dt; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0, c = 0, d = 1e300;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+      a += red[i][0]; b += red[i][1]; c += red[i][2];
+      d = red[i][3] < d ? red[i][3] : d;
+    }
+    double* o = partial + blockIdx.x * 5ll;
+    o[0] = a; o[1] = b; o[2] = c; o[3] = 0.0; o[4] = d;
+  }
+}
+
+// Deterministic reduction of n partials (fixed order, one block).
+__global__ void reduce_partials_kernel(const double* __restrict__ partial, long long n, double dt0,
+                                       double* __restrict__ out) {
+  __shared__ double red[1024][4];
+  double a = 0, b = 0, c = 0, d = 1e300;
+  for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+    a += partial[i * 5 + 0]; b += partial[i * 5 + 1]; c += partial[i * 5 + 2];
+    d = partial[i * 5 + 4] < d ? partial[i * 5 + 4] : d;
+  }
+  red[threadIdx.x][0] = a; red[threadIdx.x][1] = b; red[threadIdx.x][2] = c; red[threadIdx.x][3] = d;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      red[threadIdx.x][0] += red[threadIdx.x + s][0];
+      red[threadIdx.x][1] += red[threadIdx.x + s][1];
+      red[threadIdx.x][2] += red[threadIdx.x + s][2];
+      double o = red[threadIdx.x + s][3];
+      red[threadIdx.x][3] = o < red[threadIdx.x][3] ? o : red[threadIdx.x][3];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = red[0][0]; out[1] = red[0][1]; out[2] = red[0][2]; out[3] = 0.0;
+    out[4] = red[0][3] < dt0 ? red[0][3] : dt0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+static int check_ready(bool need_mesh = true) {
+  Context& c = ctx();
+  if (!c.inited) { set_error("rh_init has not been called"); return RH_ESTATE; }
+  if (need_mesh && !c.have_mesh) { set_error("no mesh: call rh_set_mesh first"); return RH_ESTATE; }
+  return RH_OK;
+}
+
+static int level_of_range(int head_idx, int num_octs) {
+  Context& c = ctx();
+  for (int l = c.levelmin; l <= c.levelmax; ++l)
+    if (c.noct[l] > 0 && c.head[l] == head_idx && c.noct[l] == num_octs) return l;
+  return -1;
+}
+
+static int level_of_subgrids(int head_sub, int num_sub) {
+  Context& c = ctx();
+  const int n3 = c.nsubgrid * c.nsubgrid * c.nsubgrid;
+  for (int l = c.levelmin; l <= c.levelmax; ++l)
+    if (c.noct[l] > 0 && (c.head[l] - 1) / n3 + 1 == head_sub && c.noct[l] / n3 == num_sub) return l;
+  return -1;
+}
+
+static long long total_octs() { return ctx().ngridmax; }
+
+static void free_tables(LevelTables& t) {
+  cudaFree(t.d_phdr);
+  cudaFree(t.d_poff);
+  cudaFree(t.d_ptab);
+  cudaFree(t.d_cfl_partial);
+  t = LevelTables();
+}
+
+static void free_state() {
+  Context& c = ctx();
+  for (auto& t : c.levels) free_tables(t);
+  c.levels.clear();
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(c.ud[i]);
+    cudaFree(c.uf[i]);
+    c.ud[i] = nullptr;
+    c.uf[i] = nullptr;
+  }
+  cudaFree(c.d_cfl);
+  cudaFree(c.d_scratch);
+  c.d_cfl = nullptr;
+  c.d_scratch = nullptr;
+  c.scratch_elems = 0;
+  c.have_mesh = false;
+}
+
+// Oct index (0-based) at level-l oct coordinates, after periodic wrap /
+// non-periodic clamp (zero-gradient and reflexive ghosts both take their
+// cells from the adjacent interior oct: amr/boundaries.f90:150-216).
+static inline long long wrap_clamp(long long v, long long n, int periodic) {
+  if (periodic) {
+    v %= n;
+    if (v < 0) v += n;
+    return v;
+  }
+  return v < 0 ? 0 : (v >= n ? n - 1 : v);
+}
+
+// Build the pencil tables of a complete (uniform) level.
+static int build_level_tables(int l, const TileCfg& cfg) {
+  Context& c = ctx();
+  LevelTables& T = c.levels[l];
+  free_tables(T);
+  T.cfg = cfg;
+  const long long nx = (long long)c.box_nx[0] << (l - 1), ny = (long long)c.box_nx[1] << (l - 1),
+                  nz = (long long)c.box_nx[2] << (l - 1);
+  T.nxo = (int)nx;
+  T.nyo = (int)ny;
+  T.nzo = (int)nz;
+  if ((long long)c.noct[l] != nx * ny * nz) {
+    set_error("level %d has %d octs, its box holds %lld: coarse-fine levels need the AMR table builder", l,
+              c.noct[l], nx * ny * nz);
+    return RH_EINVAL;
+  }
+  std::vector<int> idx((size_t)(nx * ny * nz), -1);
+  for (int i = 0; i < c.noct[l]; ++i) {
+    const rh_oct& o = c.grid[(size_t)c.head[l] - 1 + i];
+    long long x = o.ckey[0], y = o.ckey[1], z = o.ckey[2];
+    if (o.lev != l || x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) {
+      set_error("oct %d of level %d has key (%lld,%lld,%lld) outside its box", c.head[l] + i, l, x, y, z);
+      return RH_EINVAL;
+    }
+    size_t k = (size_t)((z * ny + y) * nx + x);
+    if (idx[k] >= 0) {
+      set_error("duplicate oct key at level %d", l);
+      return RH_EINVAL;
+    }
+    idx[k] = c.head[l] - 1 + i;
+  }
+  const int OW = cfg.txo + 2, OH = cfg.tyo + 2, NS = OW * OH;
+  const long long tx = (nx + cfg.txo - 1) / cfg.txo, ty = (ny + cfg.tyo - 1) / cfg.tyo,
+                  tz = (nz + cfg.lz - 1) / cfg.lz;
+  T.phdr.clear();
+  T.poff.clear();
+  T.ptab.clear();
+  for (long long bz = 0; bz < tz; ++bz)
+    for (long long by = 0; by < ty; ++by)
+      for (long long bx = 0; bx < tx; ++bx) {
+        const int ox0 = (int)(bx * cfg.txo), oy0 = (int)(by * cfg.tyo), oz0 = (int)(bz * cfg.lz);
+        const int L = (int)std::min<long long>(cfg.lz, nz - oz0);
+        T.phdr.push_back(make_int4(ox0, oy0, oz0, L));
+        T.poff.push_back((long long)T.ptab.size());
+        for (int r = 0; r < L + 2; ++r) {
+          const long long z = wrap_clamp(oz0 - 1 + r, nz, c.periodic[2]);
+          for (int j = 0; j < OH; ++j) {
+            const long long y = wrap_clamp(oy0 - 1 + j, ny, c.periodic[1]);
+            for (int i = 0; i < OW; ++i) {
+              const long long x = wrap_clamp(ox0 - 1 + i, nx, c.periodic[0]);
+              T.ptab.push_back(idx[(size_t)((z * ny + y) * nx + x)]);
+            }
+          }
+        }
+      }
+  T.npencil = (int)T.phdr.size();
+  RH_CUDA(cudaMalloc(&T.d_phdr, sizeof(int4) * T.phdr.size()));
+  RH_CUDA(cudaMalloc(&T.d_poff, sizeof(long long) * T.poff.size()));
+  RH_CUDA(cudaMalloc(&T.d_ptab, sizeof(int) * T.ptab.size()));
+  RH_CUDA(cudaMalloc(&T.d_cfl_partial, sizeof(double) * 5 * T.npencil));
+  RH_CUDA(cudaMemcpyAsync(T.d_phdr, T.phdr.data(), sizeof(int4) * T.phdr.size(), cudaMemcpyHostToDevice, c.stream));
+  RH_CUDA(cudaMemcpyAsync(T.d_poff, T.poff.data(), sizeof(long long) * T.poff.size(), cudaMemcpyHostToDevice,
+                          c.stream));
+  RH_CUDA(cudaMemcpyAsync(T.d_ptab, T.ptab.data(), sizeof(int) * T.ptab.size(), cudaMemcpyHostToDevice, c.stream));
+  RH_CUDA(cudaStreamSynchronize(c.stream));
+  T.built = true;
+  T.complete = true;
+  (void)NS;
+  return RH_OK;
+}
+
+static int upload_uold(const double* uold) {
+  Context& c = ctx();
+  const long long n = total_octs();
+  if (c.precision == RH_PREC_FP64) {
+    RH_CUDA(cudaMemcpyAsync(c.ud[c.cur], uold, sizeof(double) * 40 * n, cudaMemcpyHostToDevice, c.stream));
+  } else {
+    double* tmp = nullptr;
+    RH_CUDA(cudaMalloc(&tmp, sizeof(double) * 40 * n));
+    RH_CUDA(cudaMemcpyAsync(tmp, uold, sizeof(double) * 40 * n, cudaMemcpyHostToDevice, c.stream));
+    const long long tot = n * 40;
+    pack_bulk_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, c.stream>>>(tmp, c.uf[c.cur], c.ud[c.cur], n);
+    RH_CUDA(cudaGetLastError());
+    RH_CUDA(cudaStreamSynchronize(c.stream));
+    cudaFree(tmp);
+  }
+  RH_CUDA(cudaStreamSynchronize(c.stream));
+  std::fill(c.cfl_on_unew.begin(), c.cfl_on_unew.end(), 0);
+  std::fill(c.cfl_on_uold.begin(), c.cfl_on_uold.end(), 0);
+  return RH_OK;
+}
+
+static CflConst make_cfl(double dx, double gamma, double smallr, double smallc, double courant,
+                         const double* g) {
+  CflConst C;
+  C.gamma = gamma;
+  C.gm1 = gamma - 1.0;
+  C.smallr = smallr;
+  C.smallp = smallc * smallc / gamma;
+  C.cdx_smallc = courant * dx / smallc;
+  C.two_cdx = 2.0 * courant * dx;
+  C.two_c = 2.0 * courant;
+  double gs = 0;
+  for (int d = 0; d < 3; ++d) gs += std::fabs(g ? g[d] : 0.0);
+  C.gsum_dx = gs * dx;
+  C.ndim = 3;
+  return C;
+}
+
+}  // namespace rh
+
+using namespace rh;
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* rh_last_error(void) { return g_err.c_str(); }
+
+int rh_init(int device_ordinal) {
+  Context& c = ctx();
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    set_error("no CUDA device: %s", cudaGetErrorString(e));
+    return RH_ENODEV;
+  }
+  if (device_ordinal < 0 || device_ordinal >= n) {
+    set_error("device %d out of range (%d devices)", device_ordinal, n);
+    return RH_EINVAL;
+  }
+  if (c.inited) {
+    if (c.device == device_ordinal) return RH_OK;
+    rh_finalize();
+  }
+  RH_CUDA(cudaSetDevice(device_ordinal));
+  cudaDeviceProp prop;
+  RH_CUDA(cudaGetDeviceProperties(&prop, device_ordinal));
+  if (prop.major != 10) {
+    set_error("device %d is sm_%d%d; this library is built for sm_100a (B200)", device_ordinal, prop.major,
+              prop.minor);
+    return RH_ENODEV;
+  }
+  c.device = device_ordinal;
+  c.sm_count = prop.multiProcessorCount;
+  RH_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+  RH_CUDA(cudaMalloc(&c.d_err, sizeof(int)));
+  RH_CUDA(cudaMemset(c.d_err, 0, sizeof(int)));
+  RH_CUDA(cudaEventCreate(&c.ev0));
+  RH_CUDA(cudaEventCreate(&c.ev1));
+  c.inited = true;
+  return RH_OK;
+}
+
+int rh_finalize(void) {
+  Context& c = ctx();
+  if (!c.inited) return RH_OK;
+  cudaStreamSynchronize(c.stream);
+  free_state();
+  cudaFree(c.d_err);
+  cudaEventDestroy(c.ev0);
+  cudaEventDestroy(c.ev1);
+  cudaStreamDestroy(c.stream);
+  c = Context();
+  return RH_OK;
+}
+
+int rh_sync(void) {
+  int rc = check_ready(false);
+  if (rc) return rc;
+  Context& c = ctx();
+  RH_CUDA(cudaStreamSynchronize(c.stream));
+  int err = 0;
+  RH_CUDA(cudaMemcpy(&err, c.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    cudaMemset(c.d_err, 0, sizeof(int));
+    set_error("device wait bound exceeded (error word %d)", err);
+    return RH_ETIMEDOUT;
+  }
+  return RH_OK;
+}
+
+int rh_set_precision(int mode) {
+  int rc = check_ready(false);
+  if (rc) return rc;
+  if (mode != RH_PREC_FP64 && mode != RH_PREC_FP32_BULK) {
+    set_error("precision mode %d unknown", mode);
+    return RH_EINVAL;
+  }
+  Context& c = ctx();
+  if (c.have_mesh && mode != c.precision) {
+    set_error("precision must be chosen before rh_set_mesh");
+    return RH_ESTATE;
+  }
+  c.precision = mode;
+  return RH_OK;
+}
+
+int rh_set_interpolation(int interpol_var, int interpol_type) {
+  if (interpol_var < 0 || interpol_var > 1 || interpol_type < 0 || interpol_type > 3) {
+    set_error("interpol_var must be 0/1 and interpol_type 0..3");
+    return RH_EINVAL;
+  }
+  ctx().interpol_var = interpol_var;
+  ctx().interpol_type = interpol_type;
+  return RH_OK;
+}
+
+int rh_set_tile(int txo, int tyo, int lz) {
+  int rc = check_ready(false);
+  if (rc) return rc;
+  Context& c = ctx();
+  if (!find_launcher(c.precision, txo, tyo, 2, 3) || lz < 1) {
+    set_error("tile %dx%d (lz=%d) is not compiled for this precision", txo, tyo, lz);
+    return RH_EINVAL;
+  }
+  c.cfg.txo = txo;
+  c.cfg.tyo = tyo;
+  c.cfg.lz = lz;
+  if (c.have_mesh)
+    for (int l = c.levelmin; l <= c.levelmax; ++l)
+      if (c.levels[l].built) {
+        rc = build_level_tables(l, c.cfg);
+        if (rc) return rc;
+      }
+  return RH_OK;
+}
+
+int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotondim) {
+  int rc = check_ready(false);
+  if (rc) return rc;
+  Context& c = ctx();
+  if (!m || !uold || !m->grid || !m->head || !m->noct) {
+    set_error("rh_set_mesh: null pointer");
+    return RH_EINVAL;
+  }
+  if (nvar != 5 || twotondim != 8) {
+    set_error("rh_set_mesh: nvar=%d twotondim=%d; this path is NDIM=3 hydro (nvar=5, twotondim=8)", nvar,
+              twotondim);
+    return RH_EINVAL;
+  }
+  if (m->levelmin < 1 || m->levelmax < m->levelmin || m->levelmax > 24 || m->ngridmax < 1 || m->nsubgrid < 1) {
+    set_error("rh_set_mesh: bad levels/ngridmax/nsubgrid");
+    return RH_EINVAL;
+  }
+  cudaStreamSynchronize(c.stream);
+  free_state();
+  c.nsubgrid = m->nsubgrid;
+  c.levelmin = m->levelmin;
+  c.levelmax = m->levelmax;
+  c.ngridmax = m->ngridmax;
+  for (int d = 0; d < 3; ++d) {
+    c.box_nx[d] = m->box_nx[d];
+    c.periodic[d] = m->periodic[d];
+    c.gravity[d] = m->constant_gravity[d];
+  }
+  for (int i = 0; i < 6; ++i) {
+    c.bound_type[i] = m->bound_type[i];
+    const int d = i / 2;
+    if (!c.periodic[d] && c.bound_type[i] != RH_BOUND_ZERO_GRADIENT && c.bound_type[i] != RH_BOUND_REFLEXIVE) {
+      set_error("boundary %d: type %d not supported (periodic, reflexive or zero-gradient)", i, c.bound_type[i]);
+      return RH_EINVAL;
+    }
+  }
+  c.boxlen = m->boxlen;
+  c.head.assign(m->head, m->head + m->levelmax + 1);
+  c.noct.assign(m->noct, m->noct + m->levelmax + 1);
+  long long nused = 0;
+  for (int l = c.levelmin; l <= c.levelmax; ++l) {
+    if (c.noct[l] < 0 || (c.noct[l] > 0 && (c.head[l] < 1 || c.head[l] - 1 + (long long)c.noct[l] > c.ngridmax))) {
+      set_error("level %d range [%d, +%d) outside 1..ngridmax=%d", l, c.head[l], c.noct[l], c.ngridmax);
+      return RH_EINVAL;
+    }
+    nused = std::max(nused, (long long)c.head[l] - 1 + c.noct[l]);
+  }
+  c.grid.assign(m->grid, m->grid + nused);
+  const long long n = c.ngridmax;
+  for (int i = 0; i < 2; ++i) {
+    if (c.precision == RH_PREC_FP64) {
+      RH_CUDA(cudaMalloc(&c.ud[i], sizeof(double) * 40 * n));
+    } else {
+      RH_CUDA(cudaMalloc(&c.uf[i], sizeof(float) * 32 * n));
+      RH_CUDA(cudaMalloc(&c.ud[i], sizeof(double) * 8 * n));
+    }
+  }
+  RH_CUDA(cudaMalloc(&c.d_cfl, sizeof(double) * 5 * (c.levelmax + 1)));
+  c.cur = 0;
+  c.levels.assign(c.levelmax + 1, LevelTables());
+  c.unew_pending.assign(c.levelmax + 1, 0);
+  c.unew_written.assign(c.levelmax + 1, 0);
+  c.cfl_on_unew.assign(c.levelmax + 1, 0);
+  c.cfl_on_uold.assign(c.levelmax + 1, 0);
+  c.have_mesh = true;
+  rc = upload_uold(uold);
+  if (rc) return rc;
+  for (int l = c.levelmin; l <= c.levelmax; ++l) {
+    if (c.noct[l] == 0) continue;
+    rc = build_level_tables(l, c.cfg);
+    if (rc) {
+      // keep the mesh usable for set_unew/set_uold/cmpdt; godunov on this
+      // level will report the table error
+      c.levels[l].built = false;
+    }
+  }
+  return RH_OK;
+}
+
+int rh_set_grid_device(const double* uold, int ngridmax, int nvar, int twotondim) {
+  int rc = check_ready();
+  if (rc) return rc;
+  Context& c = ctx();
+  if (!uold || ngridmax != c.ngridmax || nvar != 5 || twotondim != 8) {
+    set_error("rh_set_grid_device: shape differs from the mesh (ngridmax=%d)", c.ngridmax);
+    return RH_EINVAL;
+  }
+  return upload_uold(uold);
+}
+
+int rh_transfer_grid_host(double* uold, int ngridmax, int nvar, int twotondim) {
+  int rc = check_ready();
+  if (rc) return rc;
+  Context& c = ctx();
+  if (!uold || ngridmax != c.ngridmax || nvar != 5 || twotondim != 8) {
+    set_error("rh_transfer_grid_host: shape differs from the mesh (ngridmax=%d)", c.ngridmax);
+    return RH_EINVAL;
+  }
+  const long long n = c.ngridmax;
+  if (c.precision == RH_PREC_FP64) {
+    RH_CUDA(cudaMemcpyAsync(uold, c.ud[c.cur], sizeof(double) * 40 * n, cudaMemcpyDeviceToHost, c.stream));
+  } else {
+    double* tmp = nullptr;
+    RH_CUDA(cudaMalloc(&tmp, sizeof(double) * 40 * n));
+    const long long tot = n * 40;
+    unpack_bulk_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, c.stream>>>(tmp, c.uf[c.cur], c.ud[c.cur], n);
+    RH_CUDA(cudaGetLastError());
+    RH_CUDA(cudaMemcpyAsync(uold, tmp, sizeof(double) * 40 * n, cudaMemcpyDeviceToHost, c.stream));
+    RH_CUDA(cudaStreamSynchronize(c.stream));
+    cudaFree(tmp);
+  }
+  RH_CUDA(cudaStreamSynchronize(c.stream));
+  return RH_OK;
+}
+
+// Copy a level range between the two state buffers (src -> dst).
+static int copy_level(int head_idx, int num_octs, int src, int dst) {
+  Context& c = ctx();
+  const long long o0 = head_idx - 1, n = num_octs;
+  const int threads = 256;
+  const int blocks = std::max(1, std::min(c.sm_count * 8, (int)((n * 40 + threads - 1) / threads)));
+  if (c.precision == RH_PREC_FP64) {
+    copy_kernel<double><<<blocks, threads, 0, c.stream>>>(c.ud[dst] + o0 * 40, c.ud[src] + o0 * 40, n * 40);
+  } else {
+    copy_kernel<float><<<blocks, threads, 0, c.stream>>>(c.uf[dst] + o0 * 32, c.uf[src] + o0 * 32, n * 32);
+    copy_kernel<double><<<blocks, threads, 0, c.stream>>>(c.ud[dst] + o0 * 8, c.ud[src] + o0 * 8, n * 8);
+  }
+  RH_CUDA(cudaGetLastError());
+  return RH_OK;
+}
+
+int rh_set_unew(int head_idx, int num_octs) {
+  int rc = check_ready();
+  if (rc) return rc;
+  Context& c = ctx();
+  if (num_octs == 0) return RH_OK;
+  if (head_idx < 1 || num_octs < 0 || head_idx - 1 + (long long)num_octs > c.ngridmax) {
+    set_error("rh_set_unew: range outside the mesh");
+    return RH_EINVAL;
+  }
+  const int l = level_of_range(head_idx, num_octs);
+  if (l >= 0) {
+    // unew = uold is folded into the next rh_godunov of this level, which then
+    // writes unew = uold + flux differences for every oct of the level.
+    c.unew_pending[l] = 1;
+    c.unew_written[l] = 0;
+    return RH_OK;
+  }
+  return copy_level(head_idx, num_octs, c.cur, 1 - c.cur);
+}
+
+int rh_set_uold(int head_idx, int num_octs) {
+  int rc = check_ready();
+  if (rc) return rc;
+  Context& c = ctx();
+  if (num_octs == 0) return RH_OK;
+  if (head_idx < 1 || num_octs < 0 || head_idx - 1 + (long long)num_octs > c.ngridmax) {
+    set_error("rh_set_uold: range outside the mesh");
+    return RH_EINVAL;
+  }
+  const int l = level_of_range(head_idx, num_octs);
+  if (l >= 0 && c.unew_pending[l]) {
+    // set_unew without godunov: unew == uold, nothing to copy
+    c.unew_pending[l] = 0;
+    return RH_OK;
+  }
+  // single level spanning the whole state: swap the buffers
+  int nlev = 0;
+  for (int k = c.levelmin; k <= c.levelmax; ++k) nlev += c.noct[k] > 0;
+  if (l >= 0 && nlev == 1 && c.unew_written[l]) {
+    c.cur = 1 - c.cur;
+    c.unew_written[l] = 0;
+    if (c.cfl_on_unew[l]) {
+      c.cfl_on_unew[l] = 0;
+      c.cfl_on_uold[l] = 1;
+    }
+    return RH_OK;
+  }
+  rc = copy_level(head_idx, num_octs, 1 - c.cur, c.cur);
+  if (rc) return rc;
+  if (l >= 0) {
+    c.unew_written[l] = 0;
+    c.cfl_on_uold[l] = c.cfl_on_unew[l];
+    c.cfl_on_unew[l] = 0;
+  }
+  return RH_OK;
+}
+
+int rh_cmpdt(int head_idx, int num_octs, double dx, double gamma, double smallr, double smallc,
+             double courant_factor, const double* constant_gravity, double* mass, double* ekin, double* eint,
+             double* emag, double* dt) {
+  int rc = check_ready();
+  if (rc) return rc;
+  Context& c = ctx();
+  if (!mass || !ekin || !eint || !emag || !dt) {
+    set_error("rh_cmpdt: null output pointer");
+    return RH_EINVAL;
+  }
+  if (!(dx > 0) || !(gamma > 1) || !(smallc > 0) || !(courant_factor > 0)) {
+    set_error("rh_cmpdt: need dx>0, gamma>1, smallc>0, courant_factor>0");
+    return RH_EINVAL;
+  }
+  const double g[3] = {constant_gravity ? constant_gravity[0] : 0.0, constant_gravity ? constant_gravity[1] : 0.0,
+                       constant_gravity ? constant_gravity[2] : 0.0};
+  *mass = *ekin = *eint = *emag = 0.0;
+  *dt = dx / smallc;  // courant_fine.f90:86
+  if (num_octs == 0) return RH_OK;
+  if (head_idx < 1 || num_octs < 0 || head_idx - 1 + (long long)num_octs > c.ngridmax) {
+    set_error("rh_cmpdt: range outside the mesh");
+    return RH_EINVAL;
+  }
+  const int l = level_of_range(head_idx, num_octs);
+  const double key[8] = {dx, gamma, smallr, smallc, courant_factor, g[0], g[1], g[2]};
+  const bool same_key = std::equal(key, key + 8, c.cfl_key);
+  double out[5];
+  if (l >= 0 && c.cfl_on_uold[l] && same_key) {
+    RH_CUDA(cudaMemcpyAsync(out, c.d_cfl + 5 * l, sizeof out, cudaMemcpyDeviceToHost, c.stream));
+    RH_CUDA(cudaStreamSynchronize(c.stream));
+  } else {
+    const long long ncell = (long long)num_octs * 8;
+    const int threads = 256;
+    const long long nblk = (ncell + threads - 1) / threads;
+    if ((size_t)nblk * 5 > c.scratch_elems) {
+      cudaFree(c.d_scratch);
+      c.d_scratch = nullptr;
+      RH_CUDA(cudaMalloc(&c.d_scratch, sizeof(double) * 5 * nblk));
+      c.scratch_elems = (size_t)nblk * 5;
+    }
+    // leaf mask of the level (refined flags of the grid records)
+    std::vector<uint8_t> ref((size_t)num_octs * 8);
+    bool any = false;
+    for (long long i = 0; i < num_octs; ++i)
+      for (int k = 0; k < 8; ++k) {
+        ref[i * 8 + k] = c.grid[head_idx - 1 + i].refined[k] ? 1 : 0;
+        any |= ref[i * 8 + k] != 0;
+      }
+    uint8_t* d_ref = nullptr;
+    if (any) {
+      RH_CUDA(cudaMalloc(&d_ref, ref.size()));
+      RH_CUDA(cudaMemcpyAsync(d_ref, ref.data(), ref.size(), cudaMemcpyHostToDevice, c.stream));
+    }
+    const CflConst C = make_cfl(dx, gamma, smallr, smallc, courant_factor, g);
+    const double vol = dx * dx * dx;
+    const bool fp32 = c.precision == RH_PREC_FP32_BULK;
+    cmpdt_kernel<<<(unsigned)nblk, threads, 0, c.stream>>>(c.ud[c.cur], c.uf[c.cur], fp32 ? 1 : 0, d_ref,
+                                                           head_idx - 1, num_octs, C, vol, c.d_scratch);
+    RH_CUDA(cudaGetLastError());
+    double* d_out = c.d_cfl + 5 * (l >= 0 ? l : 0);
+    reduce_partials_kernel<<<1, 1024, 0, c.stream>>>(c.d_scratch, nblk, 1e300, d_out);
+    RH_CUDA(cudaGetLastError());
+    RH_CUDA(cudaMemcpyAsync(out, d_out, sizeof out, cudaMemcpyDeviceToHost, c.stream));
+    RH_CUDA(cudaStreamSynchronize(c.stream));
+    if (d_ref) cudaFree(d_ref);
+    if (l >= 0) c.cfl_on_uold[l] = 0;
+  }
+  std::copy(key, key + 8, c.cfl_key);
+  *mass = out[0];
+  *ekin = out[1];
+  *eint = out[2];
+  *emag = 0.0;
+  *dt = std::min(*dt, out[4]);
+  return RH_OK;
+}
+
+// Launch one Godunov step of level l with the given tile configuration.
+// Exposed to the batch/bench layer through rh_godunov and rh_bench_*.
+static int launch_level(int l, double gamma, double smallr, double smallc, double dt, double dx, double smax_cap,
+                        int slope, int riemann, const double* g, bool fuse_cfl) {
+  Context& c = ctx();
+  LevelTables& T = c.levels[l];
+  if (!T.built || T.cfg.txo != c.cfg.txo || T.cfg.tyo != c.cfg.tyo || T.cfg.lz != c.cfg.lz) {
+    int rc = build_level_tables(l, c.cfg);
+    if (rc) return rc;
+  }
+  size_t smem = 0;
+  int threads = 0;
+  LaunchFn fn = find_launcher(c.precision, T.cfg.txo, T.cfg.tyo, slope, riemann, &smem, &threads);
+  if (!fn) {
+    set_error("no kernel for precision %d tile %dx%d slope %d riemann %d", c.precision, T.cfg.txo, T.cfg.tyo, slope,
+              riemann);
+    return RH_EINVAL;
+  }
+  LevelArgs A;
+  A.phdr = T.d_phdr;
+  A.poff = T.d_poff;
+  A.ptab = T.d_ptab;
+  A.npencil = T.npencil;
+  A.ncx = 2 * T.nxo;
+  A.ncy = 2 * T.nyo;
+  A.ncz = 2 * T.nzo;
+  for (int d = 0; d < 3; ++d) A.periodic[d] = c.periodic[d];
+  for (int i = 0; i < 6; ++i) A.btype[i] = c.bound_type[i];
+  A.ghost_base = c.ngridmax;
+  A.err = c.d_err;
+  const double courant = c.cfl_key[4] > 0 ? c.cfl_key[4] : smax_cap * dt / dx;
+  A.cfl = make_cfl(dx, gamma, smallr, smallc, courant, g);
+  A.vol = dx * dx * dx;
+  A.cfl_partial = fuse_cfl ? T.d_cfl_partial : nullptr;
+  const int nxt = 1 - c.cur;
+  if (c.precision == RH_PREC_FP64) {
+    StateArgs<double> S{c.ud[c.cur], nullptr, c.ud[nxt], nullptr};
+    HydroConst<double> H;
+    H.gamma = gamma; H.gm1 = gamma - 1; H.entho = 1.0 / (gamma - 1);
+    H.smallr = smallr; H.smallc = smallc; H.smallc2 = smallc * smallc;
+    H.smallp_trace = smallr * (smallc * smallc);
+    H.smallp_riem = smallc * smallc / gamma;
+    H.smalle = smallc * smallc / gamma / (gamma - 1);
+    H.dtdx = dt / dx; H.half_dtdx_unused = 0; H.smax_cap = smax_cap;
+    for (int d = 0; d < 3; ++d) H.grav_half_dt[d] = (g ? g[d] : 0.0) * (dt * 0.5);
+    RH_CUDA(fn(A, &S, &H, T.npencil, c.stream));
+  } else {
+    StateArgs<float> S{c.ud[c.cur], c.uf[c.cur], c.ud[nxt], c.uf[nxt]};
+    HydroConst<float> H;
+    H.gamma = (float)gamma; H.gm1 = (float)(gamma - 1); H.entho = (float)(1.0 / (gamma - 1));
+    H.smallr = (float)smallr; H.smallc = (float)smallc; H.smallc2 = (float)(smallc * smallc);
+    H.smallp_trace = (float)(smallr * (smallc * smallc));
+    H.smallp_riem = (float)(smallc * smallc / gamma);
+    H.smalle = (float)(smallc * smallc / gamma / (gamma - 1));
+    H.dtdx = (float)(dt / dx); H.half_dtdx_unused = 0; H.smax_cap = (float)std::min(smax_cap, 3.0e38);
+    for (int d = 0; d < 3; ++d) H.grav_half_dt[d] = (float)((g ? g[d] : 0.0) * (dt * 0.5));
+    RH_CUDA(fn(A, &S, &H, T.npencil, c.stream));
+  }
+  if (fuse_cfl) {
+    reduce_partials_kernel<<<1, 1024, 0, c.stream>>>(T.d_cfl_partial, T.npencil, A.cfl.cdx_smallc, c.d_cfl + 5 * l);
+    RH_CUDA(cudaGetLastError());
+  }
+  return RH_OK;
+}
+
+int rh_godunov(int head_idx, int num_subgrids, int ngridmax, int ilevel, int levelmin, int levelmax, double gamma,
+               double smallr, double smallc2, double dt, double dx, double smax_cap, int slope, int riemann,
+               const double* constant_gravity) {
+  int rc = check_ready();
+  if (rc) return rc;
+  Context& c = ctx();
+  if (num_subgrids == 0) return RH_OK;
+  if (ngridmax != c.ngridmax || levelmin != c.levelmin || levelmax != c.levelmax) {
+    set_error("rh_godunov: ngridmax/levelmin/levelmax differ from the mesh");
+    return RH_EINVAL;
+  }
+  const int l = level_of_subgrids(head_idx, num_subgrids);
+  if (l != ilevel) {
+    set_error("rh_godunov: subgrids [%d,+%d) are not level %d of the mesh", head_idx, num_subgrids, ilevel);
+    return RH_EINVAL;
+  }
+  if (!(dt > 0) || !(dx > 0) || !(gamma > 1) || !(smallc2 > 0)) {
+    set_error("rh_godunov: need dt>0, dx>0, gamma>1, smallc2>0");
+    return RH_EINVAL;
+  }
+  if (slope < 0 || slope > 2) {
+    set_error("rh_godunov: slope_type %d not supported on this path (0, 1 or 2)", slope);
+    return RH_EINVAL;
+  }
+  if (riemann < 1 || riemann > 3) {
+    set_error("rh_godunov: riemann %d not supported (llf=1, hll=2, hllc=3)", riemann);
+    return RH_EINVAL;
+  }
+  if (!c.unew_pending[l]) {
+    set_error("rh_godunov: call rh_set_unew for level %d first (unew must start as uold)", l);
+    return RH_ESTATE;
+  }
+  double g[3] = {0, 0, 0};
+  if (constant_gravity)
+    for (int d = 0; d < 3; ++d) g[d] = constant_gravity[d];
+  // The fused CFL epilogue uses the parameters of the last rh_cmpdt call.
+  const bool fuse = c.cfl_key[0] == dx && c.cfl_key[1] == gamma && c.cfl_key[2] == smallr &&
+                    c.cfl_key[5] == g[0] && c.cfl_key[6] == g[1] && c.cfl_key[7] == g[2] &&
+                    c.cfl_key[3] * c.cfl_key[3] == smallc2;
+  rc = launch_level(l, gamma, smallr, std::sqrt(smallc2), dt, dx, smax_cap, slope, riemann, g, fuse);
+  if (rc) return rc;
+  c.unew_pending[l] = 0;
+  c.unew_written[l] = 1;
+  c.cfl_on_unew[l] = fuse ? 1 : 0;
+  c.cfl_on_uold[l] = 0;
+  return RH_OK;
+}
+
+// ---- extensions used by the Python host layer and the bench ---------------
+
+// Device pointers of the current uold/unew buffers (for zero-copy views).
+int rh_state_ptrs(void** uold_d, void** uold_f, void** unew_d, void** unew_f) {
+  int rc = check_ready();
+  if (rc) return rc;
+  Context& c = ctx();
+  if (uold_d) *uold_d = c.ud[c.cur];
+  if (uold_f) *uold_f = c.uf[c.cur];
+  if (unew_d) *unew_d = c.ud[1 - c.cur];
+  if (unew_f) *unew_f = c.uf[1 - c.cur];
+  return RH_OK;
+}
+
+// Time n back-to-back Godunov steps of a level on device (CUDA events on the
+// library stream); dt fixed.  Returns the average milliseconds per launch.
+int rh_bench_godunov(int ilevel, int nrep, double gamma, double smallr, double smallc, double dt, double dx,
+                     double courant, int slope, int riemann, float* ms_per_step) {
+  int rc = check_ready();
+  if (rc) return rc;
+  Context& c = ctx();
+  if (ilevel < c.levelmin || ilevel > c.levelmax || nrep < 1) {
+    set_error("rh_bench_godunov: bad level or nrep");
+    return RH_EINVAL;
+  }
+  const double g[3] = {c.gravity[0], c.gravity[1], c.gravity[2]};
+  RH_CUDA(cudaEventRecord(c.ev0, c.stream));
+  for (int i = 0; i < nrep; ++i) {
+    rc = launch_level(ilevel, gamma, smallr, smallc, dt, dx, courant * dx / dt, slope, riemann, g, true);
+    if (rc) return rc;
+  }
+  RH_CUDA(cudaEventRecord(c.ev1, c.stream));
+  RH_CUDA(cudaEventSynchronize(c.ev1));
+  float ms = 0;
+  RH_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+  *ms_per_step = ms / nrep;
+  return rh_sync();
+}
+
+int rh_get_tile(int* txo, int* tyo, int* lz) {
+  Context& c = ctx();
+  if (txo) *txo = c.cfg.txo;
+  if (tyo) *tyo = c.cfg.tyo;
+  if (lz) *lz = c.cfg.lz;
+  return RH_OK;
+}
+
+int rh_list_tiles(int precision, int* txo, int* tyo, int max) { return list_tiles(precision, txo, tyo, max); }
+
+int rh_level_info(int ilevel, int* npencil, long long* table_entries) {
+  int rc = check_ready();
+  if (rc) return rc;
+  Context& c = ctx();
+  if (ilevel < 0 || ilevel > c.levelmax) return RH_EINVAL;
+  if (npencil) *npencil = c.levels[ilevel].npencil;
+  if (table_entries) *table_entries = (long long)c.levels[ilevel].ptab.size();
+  return RH_OK;
+}
+
+}  // extern "C"

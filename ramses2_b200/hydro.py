@@ -1,0 +1,105 @@
+"""Host-side mirror of the reference's hydro leaf calls, backed by librh_b200.so.
+
+:class:`GodunovGPU` exposes the per-level calls a RAMSES II host makes in one
+coarse step (amr/amr_step.f90:276-455) with the reference's names and argument
+meaning: ``courant_fine`` (r_courant_fine, hydro/courant_fine.f90:18-52),
+``set_unew`` / ``set_uold`` (hydro/godunov_fine.f90:84-214) and
+``godunov_fine`` (hydro/godunov_fine.f90:13-79).  Each call goes through the C
+ABI (include/ramses_hydro.h) exactly as the Fortran shim would.
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._abi import RH_PREC_FP32_BULK, RH_PREC_FP64, dptr
+from ._lib import check, lib
+
+PRECISION = {"fp64": RH_PREC_FP64, "fp32_bulk": RH_PREC_FP32_BULK, "fp32": RH_PREC_FP32_BULK}
+
+
+class GodunovGPU:
+    """One mesh resident on one B200, stepped through the C ABI."""
+
+    def __init__(self, mesh, params, precision="fp64", device=0, tile=None):
+        self.mesh = mesh
+        self.params = params
+        self.L = lib()
+        check(self.L.rh_init(device), "rh_init")
+        self.precision = PRECISION[precision] if isinstance(precision, str) else int(precision)
+        check(self.L.rh_set_precision(self.precision), "rh_set_precision")
+        if tile is not None:
+            check(self.L.rh_set_tile(*tile), "rh_set_tile")
+        check(self.L.rh_set_interpolation(params.interpol_var, params.interpol_type), "rh_set_interpolation")
+        self._desc = mesh.desc()
+        check(self.L.rh_set_mesh(C.byref(self._desc), dptr(mesh.uold), 5, 8), "rh_set_mesh")
+        g = np.ascontiguousarray(mesh.gravity, np.float64)
+        self._grav = g
+
+    # ---- reference leaf calls -------------------------------------------------
+    def courant_fine(self, ilevel):
+        """(mass, ekin, eint, emag, dt) of the leaf cells of a level."""
+        m = self.mesh
+        out = [C.c_double() for _ in range(5)]
+        P = self.params
+        check(self.L.rh_cmpdt(int(m.head[ilevel]), int(m.noct[ilevel]), m.dx(ilevel), P.gamma, P.smallr,
+                              P.smallc, P.courant_factor, dptr(self._grav), *[C.byref(o) for o in out]),
+              "rh_cmpdt")
+        return np.array([o.value for o in out])
+
+    def set_unew(self, ilevel):
+        m = self.mesh
+        check(self.L.rh_set_unew(int(m.head[ilevel]), int(m.noct[ilevel])), "rh_set_unew")
+
+    def set_uold(self, ilevel):
+        m = self.mesh
+        check(self.L.rh_set_uold(int(m.head[ilevel]), int(m.noct[ilevel])), "rh_set_uold")
+
+    def godunov_fine(self, ilevel, dt):
+        m = self.mesh
+        P = self.params
+        n3 = m.nsubgrid ** 3
+        head_sub = (int(m.head[ilevel]) - 1) // n3 + 1
+        nsub = int(m.noct[ilevel]) // n3
+        dx = m.dx(ilevel)
+        smax_cap = P.courant_factor * dx / dt
+        check(self.L.rh_godunov(head_sub, nsub, m.ngridmax, ilevel, m.levelmin, m.levelmax, P.gamma, P.smallr,
+                                P.smallc ** 2, dt, dx, smax_cap, P.slope_type, P.riemann, dptr(self._grav)),
+              "rh_godunov")
+
+    # ---- conveniences -----------------------------------------------------------
+    def step_uniform(self, dt=None):
+        """One coarse step of a single-level run in the reference's order."""
+        lev = self.mesh.levelmin
+        out = self.courant_fine(lev)
+        dtnew = min(self.mesh.dx(lev) / self.params.smallc, out[4]) if dt is None else dt
+        self.set_unew(lev)
+        self.godunov_fine(lev, dtnew)
+        self.set_uold(lev)
+        return dtnew, out
+
+    def fetch_uold(self):
+        """Device uold copied back in the reference layout (N, 5, 8)."""
+        u = np.empty_like(self.mesh.uold)
+        check(self.L.rh_transfer_grid_host(dptr(u), self.mesh.ngridmax, 5, 8), "rh_transfer_grid_host")
+        return u
+
+    def push_uold(self, u=None):
+        u = self.mesh.uold if u is None else np.ascontiguousarray(u, np.float64)
+        check(self.L.rh_set_grid_device(dptr(u), self.mesh.ngridmax, 5, 8), "rh_set_grid_device")
+
+    def sync(self):
+        check(self.L.rh_sync(), "rh_sync")
+
+    def set_tile(self, txo, tyo, lz):
+        check(self.L.rh_set_tile(txo, tyo, lz), "rh_set_tile")
+
+    def bench_godunov(self, ilevel, nrep, dt):
+        P = self.params
+        ms = C.c_float()
+        check(self.L.rh_bench_godunov(ilevel, nrep, P.gamma, P.smallr, P.smallc, dt, self.mesh.dx(ilevel),
+                                      P.courant_factor, P.slope_type, P.riemann, C.byref(ms)),
+              "rh_bench_godunov")
+        return ms.value
+
+    def close(self):
+        check(self.L.rh_finalize(), "rh_finalize")

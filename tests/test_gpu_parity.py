@@ -1,0 +1,152 @@
+"""Parity of the CUDA path (through the C ABI) with the FP64 CPU oracle.
+
+Bar (plain FP64 path): relative L1 error <= 1e-12 per conserved variable per
+step, on the same input state.  FP32-bulk path: density relative L1 <= 1e-5
+against the FP64 oracle.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from ramses2_b200._abi import HydroParams
+from ramses2_b200.hydro import GodunovGPU
+from ramses2_b200.mesh import riemann3d_state, sedov3d, turbulence3d, uniform_mesh
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-12
+TOL_FP32_RHO = 1e-5
+NTHREADS = os.cpu_count() or 1
+
+
+def rel_l1(a, b):
+    """Per-variable relative L1 of a vs b, both (N, 5, 8)."""
+    num = np.abs(a - b).sum(axis=(0, 2))
+    den = np.abs(b).sum(axis=(0, 2))
+    return num / np.where(den > 0, den, 1.0)
+
+
+def blast_state(mesh, seed, gamma):
+    """Random 3D Riemann problem + a pressure blob, so every wave family and
+    every direction is exercised."""
+    rng = np.random.default_rng(seed)
+    lev = mesh.levelmin
+    n = 2 * (1 << (lev - 1))
+    g, dense = riemann3d_state(rng, n, gamma=gamma)
+    x = (np.arange(n) + 0.5) / n
+    zz, yy, xx = np.meshgrid(x, x, x, indexing="ij")
+    blob = np.exp(-((xx - 0.3) ** 2 + (yy - 0.6) ** 2 + (zz - 0.45) ** 2) / 0.01)
+    dense[4] += 5.0 * blob * dense[4].mean()
+    mesh.from_dense(dense, lev)
+    return g
+
+
+def run_one_step(mesh, P, precision="fp64", tile=None, dt=None):
+    u0 = mesh.uold.copy()
+    o = oracle.OracleHydro(mesh, P, nthreads=NTHREADS)
+    dto, cfl_o = o.step_uniform(dt)
+    ref = mesh.uold.copy()
+    mesh.uold[:] = u0
+    gpu = GodunovGPU(mesh, P, precision=precision, tile=tile)
+    try:
+        dtg, cfl_g = gpu.step_uniform(dt)
+        out = gpu.fetch_uold()
+    finally:
+        gpu.close()
+    mesh.uold[:] = u0
+    return ref, out, (dto, cfl_o), (dtg, cfl_g)
+
+
+@pytest.mark.parametrize("riemann", ["llf", "hll", "hllc"])
+@pytest.mark.parametrize("slope", [0, 1, 2])
+def test_one_step_fp64_solvers_slopes(riemann, slope):
+    m = uniform_mesh(5, nsubgrid=2, bc="outflow")
+    g = blast_state(m, 11 + slope, 1.4)
+    P = HydroParams.make(gamma=g, courant_factor=0.8, slope_type=slope, riemann=riemann)
+    ref, out, (dto, co), (dtg, cg) = run_one_step(m, P)
+    assert dto == pytest.approx(dtg, rel=1e-13)
+    err = rel_l1(out, ref)
+    assert np.all(err <= TOL_FP64), err
+
+
+@pytest.mark.parametrize("bc", ["outflow", "periodic", "reflexive",
+                                ["periodic", "periodic", "outflow", "outflow", "reflexive", "reflexive"]])
+@pytest.mark.parametrize("tile", [(7, 7, 3), (8, 4, 2), (8, 8, 16)])
+def test_one_step_fp64_boundaries_tiles(bc, tile):
+    m = uniform_mesh(5, nsubgrid=1, bc=bc)
+    g = blast_state(m, 3, 1.6)
+    P = HydroParams.make(gamma=g, courant_factor=0.8, slope_type=2, riemann="hllc")
+    ref, out, _, _ = run_one_step(m, P, tile=tile)
+    err = rel_l1(out, ref)
+    assert np.all(err <= TOL_FP64), err
+
+
+def test_courant_fine_parity():
+    m = uniform_mesh(5, nsubgrid=2, bc="outflow")
+    g = blast_state(m, 5, 1.4)
+    P = HydroParams.make(gamma=g, courant_factor=0.8, slope_type=2, riemann="hllc")
+    o = oracle.OracleHydro(m, P).courant_fine(5)
+    gpu = GodunovGPU(m, P)
+    try:
+        c = gpu.courant_fine(5)
+    finally:
+        gpu.close()
+    assert c[0] == pytest.approx(o[0], rel=1e-12)
+    assert c[1] == pytest.approx(o[1], rel=1e-12)
+    assert c[2] == pytest.approx(o[2], rel=1e-11)
+    assert c[4] == pytest.approx(o[4], rel=1e-13)
+
+
+def test_sedov_multistep_fp64():
+    """Config-0 style Sedov (moncen, HLLC, C=0.8, outflow) at 32^3: both paths
+    evolve independently for 12 steps; every step stays within the bar and
+    the fused CFL values match the oracle's courant_fine."""
+    m = uniform_mesh(5, nsubgrid=1, bc="outflow")
+    sedov3d(m)
+    P = HydroParams.make(gamma=1.4, courant_factor=0.8, slope_type=2, riemann="hllc")
+    mo = uniform_mesh(5, nsubgrid=1, bc="outflow")
+    mo.uold[:] = m.uold
+    o = oracle.OracleHydro(mo, P, nthreads=NTHREADS)
+    gpu = GodunovGPU(m, P)
+    try:
+        for step in range(12):
+            dto, co = o.step_uniform()
+            dtg, cg = gpu.step_uniform()
+            assert dtg == pytest.approx(dto, rel=1e-12)
+            assert cg[0] == pytest.approx(co[0], rel=1e-12)
+            err = rel_l1(gpu.fetch_uold(), mo.uold)
+            assert np.all(err <= TOL_FP64), (step, err)
+    finally:
+        gpu.close()
+
+
+def test_turbulence_one_step_fp64():
+    m = uniform_mesh(5, nsubgrid=1, bc="periodic")
+    turbulence3d(m, gamma=1.001, mach=5.0)
+    P = HydroParams.make(gamma=1.001, courant_factor=0.8, slope_type=1, riemann="hllc")
+    ref, out, _, _ = run_one_step(m, P)
+    err = rel_l1(out, ref)
+    assert np.all(err <= TOL_FP64), err
+
+
+@pytest.mark.parametrize("case", ["sedov", "turb", "blast"])
+def test_one_step_fp32_bulk(case):
+    m = uniform_mesh(5, nsubgrid=1, bc="periodic" if case == "turb" else "outflow")
+    gamma = 1.4
+    slope = 2
+    if case == "sedov":
+        sedov3d(m)
+    elif case == "turb":
+        gamma = 1.001
+        slope = 1
+        turbulence3d(m, gamma=gamma, mach=5.0)
+    else:
+        gamma = blast_state(m, 9, 1.4)
+    P = HydroParams.make(gamma=gamma, courant_factor=0.8, slope_type=slope, riemann="hllc")
+    ref, out, (dto, _), (dtg, _) = run_one_step(m, P, precision="fp32_bulk")
+    assert dtg == pytest.approx(dto, rel=1e-6)
+    err = rel_l1(out, ref)
+    assert err[0] <= TOL_FP32_RHO, err
+    assert np.all(err <= 1e-4), err
