@@ -348,6 +348,7 @@ static CflConst make_cfl(double dx, double gamma, double smallr, double smallc, 
   double gs = 0;
   for (int d = 0; d < 3; ++d) gs += std::fabs(g ? g[d] : 0.0);
   C.gsum_dx = gs * dx;
+  C.k0 = C.two_cdx / (1.0 + std::sqrt(1.0 + C.two_c * 0.0001));
   C.ndim = 3;
   return C;
 }

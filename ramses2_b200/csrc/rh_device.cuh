@@ -187,6 +187,7 @@ struct CflConst {
   double two_cdx;                     // 2*courant*dx
   double two_c;                       // 2*courant
   double gsum_dx;                     // (|gx|+|gy|+|gz|)*dx
+  double k0;                          // 2*courant*dx/(1+sqrt(1+2*courant*1e-4)): dt*ctot without gravity
   int ndim;
 };
 
@@ -205,9 +206,15 @@ __device__ __forceinline__ double cmpdt_cell(double r, double mx, double my, dou
   double ctot = fabs(u) + c;
   if (C.ndim > 1) ctot += fabs(v) + c;
   if (C.ndim > 2) ctot += fabs(w) + c;
-  double grav = C.gsum_dx / (ctot * ctot);
-  grav = grav > 0.0001 ? grav : 0.0001;
-  double dtcell = C.two_cdx / (ctot * (1.0 + sqrt(1.0 + C.two_c * grav)));
+  double dtcell;
+  if (C.gsum_dx == 0.0) {
+    // grav = max(0, 1e-4): the square root is a constant of the launch
+    dtcell = C.k0 / ctot;
+  } else {
+    double grav = C.gsum_dx / (ctot * ctot);
+    grav = grav > 0.0001 ? grav : 0.0001;
+    dtcell = C.two_cdx / (ctot * (1.0 + sqrt(1.0 + C.two_c * grav)));
+  }
   return dtcell < C.cdx_smallc ? dtcell : C.cdx_smallc;
 }
 

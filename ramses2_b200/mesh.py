@@ -134,27 +134,28 @@ class Mesh:
             self.uold[sl, v, :] = dense[v, cells[..., 2], cells[..., 1], cells[..., 0]]
 
 
-def uniform_mesh(level, nsubgrid=1, boxlen=1.0, bc="outflow", gravity=(0.0, 0.0, 0.0)):
-    """A single-level mesh (levelmin = levelmax = level) over the unit box.
+def uniform_mesh(level, nsubgrid=1, boxlen=1.0, bc="outflow", gravity=(0.0, 0.0, 0.0), box_nx=(1, 1, 1)):
+    """A single-level mesh (levelmin = levelmax = level) covering its box.
 
-    Blocks of nsubgrid**3 octs are stored in Morton order of the block
-    coordinate, octs inside a block in Morton order.
+    ``box_nx`` is the box size in level-1 octs (a level-l edge holds
+    ``box_nx[d] * 2**(l-1)`` octs).  Blocks of nsubgrid**3 octs are stored in
+    Morton order of the block coordinate, octs inside a block in Morton order.
     """
-    no = 1 << (level - 1)
-    assert no % nsubgrid == 0, "octs per edge must be a multiple of nsubgrid"
-    ix, iy, iz = np.meshgrid(np.arange(no), np.arange(no), np.arange(no), indexing="ij")
+    no = [int(box_nx[d]) << (level - 1) for d in range(3)]
+    assert all(n % nsubgrid == 0 for n in no), "octs per edge must be a multiple of nsubgrid"
+    ix, iy, iz = np.meshgrid(np.arange(no[0]), np.arange(no[1]), np.arange(no[2]), indexing="ij")
     ix, iy, iz = ix.ravel(), iy.ravel(), iz.ravel()
     n = nsubgrid
     bkey = _morton3(ix // n, iy // n, iz // n)
     okey = _morton3(ix % n, iy % n, iz % n)
     order = np.lexsort((okey, bkey))
-    grid = np.zeros(no ** 3, dtype=OCT_DTYPE)
+    grid = np.zeros(len(ix), dtype=OCT_DTYPE)
     grid["ckey"][:, 0] = ix[order]
     grid["ckey"][:, 1] = iy[order]
     grid["ckey"][:, 2] = iz[order]
     grid["lev"] = level
     grid["hkey"] = _morton3(ix[order], iy[order], iz[order])
-    return Mesh(grid, level, level, nsubgrid=nsubgrid, boxlen=boxlen, bc=bc, gravity=gravity)
+    return Mesh(grid, level, level, nsubgrid=nsubgrid, boxlen=boxlen, bc=bc, gravity=gravity, box_nx=box_nx)
 
 
 # ---------------------------------------------------------------------------
