@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark: Sedov3D 256^3 hydro steps on B200, FP32-bulk vs plain FP64.
+
+Workload ("sedov3d_256"): uniform 256^3 grid (levelmin = levelmax = 8, unit
+box, zero-gradient outflow boundaries), gamma = 1.4, ambient rho = 1, v = 0,
+p = 1e-5, total energy 1 deposited as uniform pressure within 2 cells of the
+centre; MUSCL-Hancock, moncen slopes, HLLC, Courant 0.8.  Synthetic input built
+here (no dataset).  A step is one full hydro step through the C ABI in the
+reference's call order: rh_cmpdt (CFL dt + conserved totals, synchronous like
+gpu_cmpdt_2), rh_set_unew, rh_godunov, rh_set_uold.
+
+value        cell-updates/s of the FP32-bulk step (state resident in HBM)
+fp64         the same for the plain FP64 step
+e2e          FP32-bulk step with host buffers: per step rh_set_grid_device
+             from pinned host memory and rh_transfer_grid_host back
+roofline     dominant kernel (godunov_pencil_kernel), algorithmic bytes per
+             cell-update (48 B FP32-bulk, 80 B FP64) / CUDA-event kernel time
+cpu_baseline the CPU restatement of the reference path (oracle/, OpenMP over
+             oct blocks) timed on this host on one 256^3 step
+accuracy     density/momentum/energy relative L1 of one FP32-bulk step against
+             the FP64 oracle step from the same state
+
+--impl reference runs the reference arm: the reference's CPU algorithm on the
+host cores (the CPU restatement; the Fortran reference cannot be compiled in
+this image), same workload and metric.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LEVEL = 8
+B_ALG = {"fp64": 80.0, "fp32_bulk": 48.0}
+WORKLOAD = "sedov3d_256"
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(prec):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "godunov_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    e = d.get(prec)
+    return None if e is None else e.get("bytes_per_launch_256")
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def make_problem():
+    from ramses2_b200._abi import HydroParams
+    from ramses2_b200.mesh import sedov3d, uniform_mesh
+
+    m = uniform_mesh(LEVEL, nsubgrid=1, bc="outflow")
+    sedov3d(m, gamma=1.4, rho0=1.0, p0=1e-5, energy=1.0, radius_cells=2.0)
+    P = HydroParams.make(gamma=1.4, courant_factor=0.8, slope_type=2, riemann="hllc")
+    return m, P
+
+
+def rel_l1(a, b):
+    num = np.abs(a - b).sum(axis=(0, 2))
+    den = np.abs(b).sum(axis=(0, 2))
+    return (num / np.where(den > 0, den, 1.0)).tolist()
+
+
+def time_steps(gpu, lib, steps, warmup):
+    from ramses2_b200._lib import check
+    import ctypes as C
+
+    for _ in range(warmup):
+        gpu.step_uniform()
+    gpu.sync()
+    ms = C.c_float()
+    check(lib.rh_timer_start(), "rh_timer_start")
+    for _ in range(steps):
+        gpu.step_uniform()
+    check(lib.rh_timer_stop(C.byref(ms)), "rh_timer_stop")
+    gpu.sync()
+    return ms.value / steps
+
+
+def kernel_time(gpu, steps, dt):
+    gpu.bench_godunov(LEVEL, 2, dt)
+    return gpu.bench_godunov(LEVEL, max(3, steps), dt)
+
+
+def run_ours(args):
+    import ctypes as C
+
+    from ramses2_b200._lib import check, lib
+    from ramses2_b200.hydro import GodunovGPU
+
+    rank, world, local = env_rank()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist_
+
+        torch.cuda.set_device(local)
+        dist_.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist = dist_
+    device = local
+    m, P = make_problem()
+    ncell = int(m.noct[LEVEL]) * 8
+    u0 = m.uold.copy()
+    L = lib()
+    results = {}
+    kernel_ms = {}
+    first_step = {}
+    for prec in ("fp64", "fp32_bulk"):
+        m.uold[:] = u0
+        gpu = GodunovGPU(m, P, precision=prec, device=device, tile=args.tile.get(prec))
+        if dist is not None:
+            dist.barrier()
+        with ClockSampler(device) as clk:
+            ms = time_steps(gpu, L, args.steps, args.warmup)
+        results[prec] = {"ms_per_step": ms, "clocks": clk.summary()}
+        # dominant kernel, device time per launch
+        m.uold[:] = u0
+        gpu.push_uold()
+        dt, _ = gpu.step_uniform()
+        first_step[prec] = gpu.fetch_uold()
+        kernel_ms[prec] = kernel_time(gpu, args.steps, dt)
+        if prec == "fp32_bulk":
+            # end to end through the ABI with host buffers (pinned)
+            try:
+                import torch
+
+                host = torch.empty(m.uold.size, dtype=torch.float64, pin_memory=True).numpy().reshape(m.uold.shape)
+            except Exception:
+                host = np.empty_like(m.uold)
+            host[:] = u0
+            from ramses2_b200._abi import dptr
+
+            gpu.sync()
+            check(L.rh_timer_start(), "rh_timer_start")
+            for _ in range(args.steps):
+                check(L.rh_set_grid_device(dptr(host), m.ngridmax, 5, 8), "rh_set_grid_device")
+                gpu.step_uniform()
+                check(L.rh_transfer_grid_host(dptr(host), m.ngridmax, 5, 8), "rh_transfer_grid_host")
+            e2e_ms = C.c_float()
+            check(L.rh_timer_stop(C.byref(e2e_ms)), "rh_timer_stop")
+            results["e2e_ms"] = e2e_ms.value / args.steps
+            results["e2e_bytes"] = int(m.uold.nbytes)
+        gpu.close()
+    # max over ranks
+    if dist is not None:
+        import torch
+
+        t = torch.tensor([results["fp32_bulk"]["ms_per_step"], results["fp64"]["ms_per_step"],
+                          results["e2e_ms"]], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        results["fp32_bulk"]["ms_per_step"], results["fp64"]["ms_per_step"], results["e2e_ms"] = t.tolist()
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    # one FP64 oracle step from the same state: CPU baseline + accuracy
+    cpu = None
+    acc = None
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        nthreads = os.cpu_count() or 1
+        m.uold[:] = u0
+        o = oracle.OracleHydro(m, P, nthreads=nthreads)
+        t0 = time.perf_counter()
+        o.step_uniform()
+        cpu_s = time.perf_counter() - t0
+        ref = m.uold.copy()
+        cpu = {"value": ncell / cpu_s, "unit": "cell-updates/s", "cores": nthreads, "kind": "port",
+               "sample": "one full 256^3 Sedov step (courant_fine + godunov_fine, OpenMP over oct blocks) "
+                         "of the CPU restatement, %.2f s" % cpu_s}
+        acc = {"fp32_bulk_vs_fp64_oracle_rel_l1": dict(zip(["rho", "mx", "my", "mz", "E"],
+                                                           rel_l1(first_step["fp32_bulk"], ref))),
+               "fp64_vs_fp64_oracle_rel_l1": dict(zip(["rho", "mx", "my", "mz", "E"],
+                                                      rel_l1(first_step["fp64"], ref)))}
+    peak, peak_kind = measured_peaks()
+    prec = "fp32_bulk"
+    ms = results[prec]["ms_per_step"]
+    value = world * ncell / (ms * 1e-3)
+    kms = kernel_ms[prec]
+    achieved = ncell * B_ALG[prec] / (kms * 1e-3) / 1e9
+    launches = args.steps * 2  # pencil kernel + partial reduction per step (rh_cmpdt hits the fused CFL)
+    line = {
+        "metric": "cell-updates/s Sedov3D 256^3 FP32-bulk vs FP64 at L1<=1e-5; p50/p99 solve latency",
+        "value": value,
+        "unit": "cell-updates/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32+fp64(E,p,dt,sums)",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": "256^3 uniform (levelmin=levelmax=8)", "problem": "Sedov3D",
+                   "riemann": "hllc", "slope": "moncen", "courant": 0.8, "boundary": "outflow",
+                   "cells": ncell, "parallelism": "replicas" if world > 1 else "single-gpu",
+                   "l2": "state (>=805 MB) larger than L2 (126 MB); no flush needed"},
+        "fp64": {"value": world * ncell / (results["fp64"]["ms_per_step"] * 1e-3),
+                 "ms_per_step": results["fp64"]["ms_per_step"],
+                 "kernel_ms": kernel_ms["fp64"],
+                 "roofline_frac": ncell * B_ALG["fp64"] / (kernel_ms["fp64"] * 1e-3) / 1e9 / peak,
+                 "clocks": results["fp64"]["clocks"]},
+        "fp32_bulk_over_fp64": results["fp64"]["ms_per_step"] / ms,
+        "e2e": {"value": world * ncell / (results["e2e_ms"] * 1e-3), "unit": "cell-updates/s",
+                "h2d_bytes_per_step": results["e2e_bytes"], "d2h_bytes_per_step": results["e2e_bytes"]},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": profile_traffic(prec), "peak_kind": peak_kind,
+                     "kernel": "godunov_pencil_kernel<float>", "kernel_ms": kms,
+                     "bytes_per_cell_update": B_ALG[prec]},
+        "cpu_baseline": cpu,
+        "accuracy": acc,
+        "gpu_launches": launches,
+        "clocks": results[prec]["clocks"],
+    }
+    print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank, world, local = env_rank()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    m, P = make_problem()
+    ncell = int(m.noct[LEVEL]) * 8
+    nthreads = os.cpu_count() or 1
+    o = oracle.OracleHydro(m, P, nthreads=nthreads)
+    for _ in range(args.warmup):
+        o.step_uniform()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.step_uniform()
+    el = (time.perf_counter() - t0) / args.steps
+    value = ncell / el
+    line = {
+        "impl": "reference",
+        "metric": "cell-updates/s Sedov3D 256^3 FP32-bulk vs FP64 at L1<=1e-5; p50/p99 solve latency",
+        "value": value,
+        "unit": "cell-updates/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": el * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": "256^3 uniform (levelmin=levelmax=8)", "problem": "Sedov3D",
+                   "riemann": "hllc", "slope": "moncen", "courant": 0.8, "boundary": "outflow", "cells": ncell},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": nthreads, "kind": "port",
+                         "sample": "full 256^3 Sedov steps of the CPU restatement of the reference path "
+                                   "(Fortran reference not compilable in this image)"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / accuracy leg")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    args.tile = {"fp64": (8, 8, 32), "fp32_bulk": (7, 7, 16)}
+    if args.impl == "reference":
+        args.steps = min(args.steps, 3)
+        args.warmup = 1
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

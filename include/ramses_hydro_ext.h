@@ -31,6 +31,11 @@ int rh_state_ptrs(void** uold_d, void** uold_f, void** unew_d, void** unew_f);
 int rh_bench_godunov(int ilevel, int nrep, double gamma, double smallr, double smallc, double dt, double dx,
                      double courant, int slope, int riemann, float* ms_per_step);
 
+/* CUDA-event timer on the library's stream: start, then stop returns the
+ * elapsed milliseconds of everything queued in between. */
+int rh_timer_start(void);
+int rh_timer_stop(float* ms);
+
 #ifdef __cplusplus
 }
 #endif

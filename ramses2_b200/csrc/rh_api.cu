@@ -772,27 +772,33 @@ static int launch_level(int l, double gamma, double smallr, double smallc, doubl
   A.vol = dx * dx * dx;
   A.cfl_partial = fuse_cfl ? T.d_cfl_partial : nullptr;
   const int nxt = 1 - c.cur;
+  A.gm1_d = gamma - 1.0;
+  A.smalle_d = smallc * smallc / gamma / (gamma - 1.0);
+  const double gh[3] = {(g ? g[0] : 0.0) * (dt * 0.5), (g ? g[1] : 0.0) * (dt * 0.5), (g ? g[2] : 0.0) * (dt * 0.5)};
   if (c.precision == RH_PREC_FP64) {
     StateArgs<double> S{c.ud[c.cur], nullptr, c.ud[nxt], nullptr};
-    HydroConst<double> H;
-    H.gamma = gamma; H.gm1 = gamma - 1; H.entho = 1.0 / (gamma - 1);
-    H.smallr = smallr; H.smallc = smallc; H.smallc2 = smallc * smallc;
+    HydroK<double> H;
+    H.gamma = gamma; H.entho = 1.0 / (gamma - 1.0);
+    H.smallr = smallr; H.smallc2 = smallc * smallc;
     H.smallp_trace = smallr * (smallc * smallc);
     H.smallp_riem = smallc * smallc / gamma;
-    H.smalle = smallc * smallc / gamma / (gamma - 1);
-    H.dtdx = dt / dx; H.half_dtdx_unused = 0; H.smax_cap = smax_cap;
-    for (int d = 0; d < 3; ++d) H.grav_half_dt[d] = (g ? g[d] : 0.0) * (dt * 0.5);
+    H.smax_cap = smax_cap; H.dtdx = dt / dx;
+    H.zero = 0.0; H.half = 0.5; H.two = 2.0;
+    H.gm1 = gamma - 1.0; H.smalle = A.smalle_d;
+    for (int d = 0; d < 3; ++d) H.grav[d] = gh[d];
     RH_CUDA(fn(A, &S, &H, T.npencil, c.stream));
   } else {
     StateArgs<float> S{c.ud[c.cur], c.uf[c.cur], c.ud[nxt], c.uf[nxt]};
-    HydroConst<float> H;
-    H.gamma = (float)gamma; H.gm1 = (float)(gamma - 1); H.entho = (float)(1.0 / (gamma - 1));
-    H.smallr = (float)smallr; H.smallc = (float)smallc; H.smallc2 = (float)(smallc * smallc);
-    H.smallp_trace = (float)(smallr * (smallc * smallc));
-    H.smallp_riem = (float)(smallc * smallc / gamma);
-    H.smalle = (float)(smallc * smallc / gamma / (gamma - 1));
-    H.dtdx = (float)(dt / dx); H.half_dtdx_unused = 0; H.smax_cap = (float)std::min(smax_cap, 3.0e38);
-    for (int d = 0; d < 3; ++d) H.grav_half_dt[d] = (float)((g ? g[d] : 0.0) * (dt * 0.5));
+    HydroK<float2> H;
+    auto b = [](double v) { float f = (float)v; return make_float2(f, f); };
+    H.gamma = b(gamma); H.entho = b(1.0 / (gamma - 1.0));
+    H.smallr = b(smallr); H.smallc2 = b(smallc * smallc);
+    H.smallp_trace = b(smallr * (smallc * smallc));
+    H.smallp_riem = b(smallc * smallc / gamma);
+    H.smax_cap = b(std::min(smax_cap, 3.0e38)); H.dtdx = b(dt / dx);
+    H.zero = b(0.0); H.half = b(0.5); H.two = b(2.0);
+    H.gm1 = b(gamma - 1.0); H.smalle = b(A.smalle_d);
+    for (int d = 0; d < 3; ++d) H.grav[d] = b(gh[d]);
     RH_CUDA(fn(A, &S, &H, T.npencil, c.stream));
   }
   if (fuse_cfl) {
@@ -887,6 +893,23 @@ int rh_bench_godunov(int ilevel, int nrep, double gamma, double smallr, double s
   RH_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
   *ms_per_step = ms / nrep;
   return rh_sync();
+}
+
+// CUDA-event timer on the library stream (brackets any sequence of calls).
+int rh_timer_start(void) {
+  int rc = check_ready(false);
+  if (rc) return rc;
+  RH_CUDA(cudaEventRecord(ctx().ev0, ctx().stream));
+  return RH_OK;
+}
+int rh_timer_stop(float* ms) {
+  int rc = check_ready(false);
+  if (rc) return rc;
+  Context& c = ctx();
+  RH_CUDA(cudaEventRecord(c.ev1, c.stream));
+  RH_CUDA(cudaEventSynchronize(c.ev1));
+  RH_CUDA(cudaEventElapsedTime(ms, c.ev0, c.ev1));
+  return RH_OK;
 }
 
 int rh_get_tile(int* txo, int* tyo, int* lz) {

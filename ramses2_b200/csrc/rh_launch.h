@@ -3,9 +3,11 @@
 #include <cuda_runtime.h>
 
 #include "rh_godunov.cuh"
+#include "rh_godunov2.cuh"
 
 namespace rh {
 
+// S: StateArgs<T>*, H: HydroK<V>* of the kernel's precision.
 using LaunchFn = cudaError_t (*)(const LevelArgs& A, const void* S, const void* H, int nblocks, cudaStream_t st);
 
 struct KernelKey {
@@ -18,30 +20,54 @@ LaunchFn find_launcher(int prec, int txo, int tyo, int slope, int riemann, size_
 // All registered tile shapes of a precision (for the autotuner).
 int list_tiles(int prec, int* txo, int* tyo, int max);
 
-template <typename T, int TXO, int TYO, int SLOPE, int RIEMANN>
-cudaError_t launch_pencil(const LevelArgs& A, const void* S, const void* H, int nblocks, cudaStream_t st) {
-  using G = Geo<T, TXO, TYO>;
-  auto k = godunov_pencil_kernel<T, TXO, TYO, SLOPE, RIEMANN>;
+template <int TXO, int TYO, int SLOPE, int RIEMANN>
+cudaError_t launch_f64(const LevelArgs& A, const void* S, const void* H, int nblocks, cudaStream_t st) {
+  using G = Geo<double, double, TXO, TYO>;
+  auto k = godunov_pencil_kernel<double, TXO, TYO, SLOPE, RIEMANN>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::kSmem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  k<<<nblocks, G::NT, G::kSmem, st>>>(A, *static_cast<const StateArgs<T>*>(S),
-                                      *static_cast<const HydroConst<T>*>(H));
+  k<<<nblocks, G::NT, G::kSmem, st>>>(A, *static_cast<const StateArgs<double>*>(S),
+                                      *static_cast<const HydroK<double>*>(H));
+  return cudaGetLastError();
+}
+
+template <int TXO, int TYO, int SLOPE, int RIEMANN>
+cudaError_t launch_f32x2(const LevelArgs& A, const void* S, const void* H, int nblocks, cudaStream_t st) {
+  using G = Geo<float, float2, TXO, TYO>;
+  auto k = godunov_pencil2_kernel<TXO, TYO, SLOPE, RIEMANN>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::kSmem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k<<<nblocks, G::NT, G::kSmem, st>>>(A, *static_cast<const StateArgs<float>*>(S),
+                                      *static_cast<const HydroK<float2>*>(H));
   return cudaGetLastError();
 }
 
 template <typename T, int TXO, int TYO> struct TileRegistrar {
   TileRegistrar() {
-    constexpr int P = sizeof(T) == 8 ? RH_PREC_FP64 : RH_PREC_FP32_BULK;
-    using G = Geo<T, TXO, TYO>;
-#define RH_REG(S, R) register_launcher({P, TXO, TYO, S, R}, &launch_pencil<T, TXO, TYO, S, R>, G::kSmem, G::NT);
-    RH_REG(0, 1) RH_REG(0, 2) RH_REG(0, 3)
-    RH_REG(1, 1) RH_REG(1, 2) RH_REG(1, 3)
-    RH_REG(2, 1) RH_REG(2, 2) RH_REG(2, 3)
+    if constexpr (sizeof(T) == 8) {
+      using G = Geo<double, double, TXO, TYO>;
+#define RH_REG(S, R) register_launcher({RH_PREC_FP64, TXO, TYO, S, R}, &launch_f64<TXO, TYO, S, R>, G::kSmem, G::NT);
+      RH_REG(0, 1) RH_REG(0, 2) RH_REG(0, 3)
+      RH_REG(1, 1) RH_REG(1, 2) RH_REG(1, 3)
+      RH_REG(2, 1) RH_REG(2, 2) RH_REG(2, 3)
 #undef RH_REG
+    } else {
+      using G = Geo<float, float2, TXO, TYO>;
+#define RH_REG(S, R) \
+  register_launcher({RH_PREC_FP32_BULK, TXO, TYO, S, R}, &launch_f32x2<TXO, TYO, S, R>, G::kSmem, G::NT);
+      RH_REG(0, 1) RH_REG(0, 2) RH_REG(0, 3)
+      RH_REG(1, 1) RH_REG(1, 2) RH_REG(1, 3)
+      RH_REG(2, 1) RH_REG(2, 2) RH_REG(2, 3)
+#undef RH_REG
+    }
   }
 };
 
