@@ -15,12 +15,13 @@
 extern "C" {
 #endif
 
-/* Pencil tile of the Godunov kernel: txo x tyo octs in x,y and lz oct layers
- * per pencil.  Only compiled tile shapes are accepted (rh_list_tiles). */
-int rh_set_tile(int txo, int tyo, int lz);
-int rh_get_tile(int* txo, int* tyo, int* lz);
+/* Pencil tile of the Godunov kernel: txo x tyo octs in x,y, registers sized
+ * for minb CTAs per SM, lz oct layers per pencil.  Only compiled shapes are
+ * accepted (rh_list_tiles). */
+int rh_set_tile(int txo, int tyo, int minb, int lz);
+int rh_get_tile(int* txo, int* tyo, int* minb, int* lz);
 /* Compiled tile shapes of a precision mode; returns their count. */
-int rh_list_tiles(int precision, int* txo, int* tyo, int max);
+int rh_list_tiles(int precision, int* txo, int* tyo, int* minb, int max);
 /* Pencil count and oct-table size of a level's current tables. */
 int rh_level_info(int ilevel, int* npencil, long long* table_entries);
 /* Device pointers of the current uold / unew buffers (FP64: *_d is

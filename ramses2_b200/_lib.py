@@ -33,9 +33,9 @@ SIGNATURES = {
     "rh_godunov": (_i, [_i, _i, _i, _i, _i, _i, _d, _d, _d, _d, _d, _d, _i, _i, _P(_d)]),
     "rh_set_interpolation": (_i, [_i, _i]),
     # extensions (include/ramses_hydro_ext.h)
-    "rh_set_tile": (_i, [_i, _i, _i]),
-    "rh_get_tile": (_i, [_P(_i), _P(_i), _P(_i)]),
-    "rh_list_tiles": (_i, [_i, _P(_i), _P(_i), _i]),
+    "rh_set_tile": (_i, [_i, _i, _i, _i]),
+    "rh_get_tile": (_i, [_P(_i), _P(_i), _P(_i), _P(_i)]),
+    "rh_list_tiles": (_i, [_i, _P(_i), _P(_i), _P(_i), _i]),
     "rh_level_info": (_i, [_i, _P(_i), _P(C.c_longlong)]),
     "rh_state_ptrs": (_i, [_P(C.c_void_p), _P(C.c_void_p), _P(C.c_void_p), _P(C.c_void_p)]),
     "rh_bench_godunov": (_i, [_i, _i, _d, _d, _d, _d, _d, _d, _i, _i, _P(C.c_float)]),

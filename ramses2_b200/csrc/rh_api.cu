@@ -54,20 +54,25 @@ static std::vector<RegEntry>& registry() {
 void register_launcher(const KernelKey& k, LaunchFn fn, size_t smem, int threads) {
   registry().push_back({k, fn, smem, threads});
 }
-LaunchFn find_launcher(int prec, int txo, int tyo, int slope, int riemann, size_t* smem, int* threads) {
+LaunchFn find_launcher(int prec, int txo, int tyo, int minb, int slope, int riemann, size_t* smem, int* threads) {
   for (auto& e : registry())
-    if (e.k.prec == prec && e.k.txo == txo && e.k.tyo == tyo && e.k.slope == slope && e.k.riemann == riemann) {
+    if (e.k.prec == prec && e.k.txo == txo && e.k.tyo == tyo && e.k.minb == minb && e.k.slope == slope &&
+        e.k.riemann == riemann) {
       if (smem) *smem = e.smem;
       if (threads) *threads = e.threads;
       return e.fn;
     }
   return nullptr;
 }
-int list_tiles(int prec, int* txo, int* tyo, int max) {
+int list_tiles(int prec, int* txo, int* tyo, int* minb, int max) {
   int n = 0;
   for (auto& e : registry()) {
     if (e.k.prec != prec || e.k.slope != 2 || e.k.riemann != 3) continue;
-    if (n < max) { txo[n] = e.k.txo; tyo[n] = e.k.tyo; }
+    if (n < max) {
+      txo[n] = e.k.txo;
+      tyo[n] = e.k.tyo;
+      minb[n] = e.k.minb;
+    }
     ++n;
   }
   return n;
@@ -453,16 +458,17 @@ int rh_set_interpolation(int interpol_var, int interpol_type) {
   return RH_OK;
 }
 
-int rh_set_tile(int txo, int tyo, int lz) {
+int rh_set_tile(int txo, int tyo, int minb, int lz) {
   int rc = check_ready(false);
   if (rc) return rc;
   Context& c = ctx();
-  if (!find_launcher(c.precision, txo, tyo, 2, 3) || lz < 1) {
-    set_error("tile %dx%d (lz=%d) is not compiled for this precision", txo, tyo, lz);
+  if (!find_launcher(c.precision, txo, tyo, minb, 2, 3) || lz < 1) {
+    set_error("tile %dx%d (minb=%d, lz=%d) is not compiled for this precision", txo, tyo, minb, lz);
     return RH_EINVAL;
   }
   c.cfg.txo = txo;
   c.cfg.tyo = tyo;
+  c.cfg.minb = minb;
   c.cfg.lz = lz;
   if (c.have_mesh)
     for (int l = c.levelmin; l <= c.levelmax; ++l)
@@ -749,10 +755,10 @@ static int launch_level(int l, double gamma, double smallr, double smallc, doubl
   }
   size_t smem = 0;
   int threads = 0;
-  LaunchFn fn = find_launcher(c.precision, T.cfg.txo, T.cfg.tyo, slope, riemann, &smem, &threads);
+  LaunchFn fn = find_launcher(c.precision, T.cfg.txo, T.cfg.tyo, c.cfg.minb, slope, riemann, &smem, &threads);
   if (!fn) {
-    set_error("no kernel for precision %d tile %dx%d slope %d riemann %d", c.precision, T.cfg.txo, T.cfg.tyo, slope,
-              riemann);
+    set_error("no kernel for precision %d tile %dx%d (minb %d) slope %d riemann %d", c.precision, T.cfg.txo,
+              T.cfg.tyo, c.cfg.minb, slope, riemann);
     return RH_EINVAL;
   }
   LevelArgs A;
@@ -912,15 +918,18 @@ int rh_timer_stop(float* ms) {
   return RH_OK;
 }
 
-int rh_get_tile(int* txo, int* tyo, int* lz) {
+int rh_get_tile(int* txo, int* tyo, int* minb, int* lz) {
   Context& c = ctx();
   if (txo) *txo = c.cfg.txo;
   if (tyo) *tyo = c.cfg.tyo;
+  if (minb) *minb = c.cfg.minb;
   if (lz) *lz = c.cfg.lz;
   return RH_OK;
 }
 
-int rh_list_tiles(int precision, int* txo, int* tyo, int max) { return list_tiles(precision, txo, tyo, max); }
+int rh_list_tiles(int precision, int* txo, int* tyo, int* minb, int max) {
+  return list_tiles(precision, txo, tyo, minb, max);
+}
 
 int rh_level_info(int ilevel, int* npencil, long long* table_entries) {
   int rc = check_ready();

@@ -291,8 +291,8 @@ __device__ __forceinline__ void ctoprim_f64(const double* sd, int cell, bool fx,
   q[4] = H.gm1 * eint;
 }
 
-template <typename T, int TXO, int TYO, int SLOPE, int RIEMANN>
-__global__ void __launch_bounds__(Geo<T, double, TXO, TYO>::NT, 1)
+template <typename T, int TXO, int TYO, int MINB, int SLOPE, int RIEMANN>
+__global__ void __launch_bounds__(Geo<T, double, TXO, TYO>::NT, MINB)
 godunov_pencil_kernel(const LevelArgs A, const StateArgs<T> S, const HydroK<double> H) {
   using G = Geo<T, double, TXO, TYO>;
   extern __shared__ __align__(16) unsigned char smem[];

@@ -50,8 +50,8 @@ __device__ __forceinline__ void ctoprim_f32x2(const float* sf, const double* sd,
   q[4] = make_float2((float)(gm1 * e0), (float)(gm1 * e1));
 }
 
-template <int TXO, int TYO, int SLOPE, int RIEMANN>
-__global__ void __launch_bounds__(Geo<float, float2, TXO, TYO>::NT, 1)
+template <int TXO, int TYO, int MINB, int SLOPE, int RIEMANN>
+__global__ void __launch_bounds__(Geo<float, float2, TXO, TYO>::NT, MINB)
 godunov_pencil2_kernel(const LevelArgs A, const StateArgs<float> S, const HydroK<float2> H) {
   using G = Geo<float, float2, TXO, TYO>;
   extern __shared__ __align__(16) unsigned char smem[];

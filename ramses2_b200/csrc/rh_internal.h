@@ -21,8 +21,9 @@ int cuda_fail(cudaError_t e, const char* what);
 
 // Tile configuration of the pencil kernel (chosen by the autotuner).
 struct TileCfg {
-  int txo = 7, tyo = 7;  // XY tile in octs
-  int lz = 16;           // oct layers per pencil
+  int txo = 8, tyo = 8;  // XY tile in octs
+  int minb = 1;          // CTAs per SM the kernel's registers are sized for
+  int lz = 32;           // oct layers per pencil
 };
 
 // Pencil tables of one level (device + host copies).

@@ -28,7 +28,7 @@ class GodunovGPU:
         self.precision = PRECISION[precision] if isinstance(precision, str) else int(precision)
         check(self.L.rh_set_precision(self.precision), "rh_set_precision")
         if tile is not None:
-            check(self.L.rh_set_tile(*tile), "rh_set_tile")
+            self.set_tile(*tile)
         check(self.L.rh_set_interpolation(params.interpol_var, params.interpol_type), "rh_set_interpolation")
         self._desc = mesh.desc()
         check(self.L.rh_set_mesh(C.byref(self._desc), dptr(mesh.uold), 5, 8), "rh_set_mesh")
@@ -90,8 +90,21 @@ class GodunovGPU:
     def sync(self):
         check(self.L.rh_sync(), "rh_sync")
 
-    def set_tile(self, txo, tyo, lz):
-        check(self.L.rh_set_tile(txo, tyo, lz), "rh_set_tile")
+    def set_tile(self, txo, tyo, lz, minb=None):
+        """Pencil tile (txo x tyo octs, lz layers); minb defaults to the
+        compiled variant with the most CTAs per SM for this shape."""
+        if minb is None:
+            opts = [b for (x, y, b) in self.tiles() if (x, y) == (txo, tyo)]
+            if not opts:
+                raise ValueError("tile %dx%d not compiled" % (txo, tyo))
+            minb = max(opts)
+        check(self.L.rh_set_tile(txo, tyo, minb, lz), "rh_set_tile")
+
+    def tiles(self):
+        """Compiled (txo, tyo, minb) shapes of this precision."""
+        tx, ty, mb = (C.c_int * 64)(), (C.c_int * 64)(), (C.c_int * 64)()
+        n = self.L.rh_list_tiles(self.precision, tx, ty, mb, 64)
+        return [(tx[i], ty[i], mb[i]) for i in range(min(n, 64))]
 
     def bench_godunov(self, ilevel, nrep, dt):
         P = self.params

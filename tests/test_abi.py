@@ -53,8 +53,10 @@ def test_ext_tile_registry_lists_compiled_shapes():
     L = lib()
     tx = (C.c_int * 16)()
     ty = (C.c_int * 16)()
-    n = L.rh_list_tiles(0, tx, ty, 16)
+    mb = (C.c_int * 16)()
+    n = L.rh_list_tiles(0, tx, ty, mb, 16)
     shapes = {(tx[i], ty[i]) for i in range(min(n, 16))}
     assert (7, 7) in shapes and (8, 8) in shapes
-    n32 = L.rh_list_tiles(1, tx, ty, 16)
+    n32 = L.rh_list_tiles(1, tx, ty, mb, 16)
     assert n32 >= 3
+    assert {mb[i] for i in range(min(n32, 16))} >= {1, 2}
