@@ -134,19 +134,23 @@ def rel_l1(a, b):
 
 
 def time_steps(gpu, lib, steps, warmup):
+    """Per-step device time (CUDA events on the library stream); every step
+    already ends with the synchronous dt read-back of rh_cmpdt."""
     from ramses2_b200._lib import check
     import ctypes as C
 
     for _ in range(warmup):
         gpu.step_uniform()
     gpu.sync()
+    per = []
     ms = C.c_float()
-    check(lib.rh_timer_start(), "rh_timer_start")
     for _ in range(steps):
+        check(lib.rh_timer_start(), "rh_timer_start")
         gpu.step_uniform()
-    check(lib.rh_timer_stop(C.byref(ms)), "rh_timer_stop")
+        check(lib.rh_timer_stop(C.byref(ms)), "rh_timer_stop")
+        per.append(ms.value)
     gpu.sync()
-    return ms.value / steps
+    return float(np.sum(per)) / steps, per
 
 
 def kernel_time(gpu, steps, dt):
@@ -157,6 +161,7 @@ def kernel_time(gpu, steps, dt):
 def run_ours(args):
     import ctypes as C
 
+    from ramses2_b200 import autotune
     from ramses2_b200._lib import check, lib
     from ramses2_b200.hydro import GodunovGPU
 
@@ -177,14 +182,20 @@ def run_ours(args):
     results = {}
     kernel_ms = {}
     first_step = {}
+    tuned = {}
     for prec in ("fp64", "fp32_bulk"):
         m.uold[:] = u0
-        gpu = GodunovGPU(m, P, precision=prec, device=device, tile=args.tile.get(prec))
+        gpu = GodunovGPU(m, P, precision=prec, device=device)
+        dt0, _ = gpu.step_uniform()
+        best, _ = autotune.tune(gpu, LEVEL, dt0)
+        tuned[prec] = best
+        m.uold[:] = u0
+        gpu.push_uold()
         if dist is not None:
             dist.barrier()
         with ClockSampler(device) as clk:
-            ms = time_steps(gpu, L, args.steps, args.warmup)
-        results[prec] = {"ms_per_step": ms, "clocks": clk.summary()}
+            ms, per = time_steps(gpu, L, args.steps, args.warmup)
+        results[prec] = {"ms_per_step": ms, "clocks": clk.summary(), "per_step": per}
         # dominant kernel, device time per launch
         m.uold[:] = u0
         gpu.push_uold()
@@ -277,6 +288,9 @@ def run_ours(args):
                  "roofline_frac": ncell * B_ALG["fp64"] / (kernel_ms["fp64"] * 1e-3) / 1e9 / peak,
                  "clocks": results["fp64"]["clocks"]},
         "fp32_bulk_over_fp64": results["fp64"]["ms_per_step"] / ms,
+        "step_latency_ms": {"p50": float(np.percentile(results[prec]["per_step"], 50)),
+                            "p99": float(np.percentile(results[prec]["per_step"], 99))},
+        "tile": {k: v for k, v in tuned.items()},
         "e2e": {"value": world * ncell / (results["e2e_ms"] * 1e-3), "unit": "cell-updates/s",
                 "h2d_bytes_per_step": results["e2e_bytes"], "d2h_bytes_per_step": results["e2e_bytes"]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -345,7 +359,6 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / accuracy leg")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
-    args.tile = {"fp64": (8, 8, 32), "fp32_bulk": (7, 7, 16)}
     if args.impl == "reference":
         args.steps = min(args.steps, 3)
         args.warmup = 1

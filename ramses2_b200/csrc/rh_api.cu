@@ -898,6 +898,10 @@ int rh_bench_godunov(int ilevel, int nrep, double gamma, double smallr, double s
   float ms = 0;
   RH_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
   *ms_per_step = ms / nrep;
+  // the timing loop overwrote unew and the level's reduced CFL values
+  c.cfl_on_unew[ilevel] = 0;
+  c.cfl_on_uold[ilevel] = 0;
+  c.unew_written[ilevel] = 0;
   return rh_sync();
 }
 
