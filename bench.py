@@ -68,53 +68,56 @@ def profile_traffic(prec):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clock and throttle reasons sampled (read-only NVML queries, every
+    ~5 ms) while the timed region runs; falls back to nvidia-smi polling."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+               "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+               "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+               "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
 
     def __init__(self, device):
         self.device = device
-        self.rows = []
-        self.proc = None
+        self.sm = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self.t = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml as N
+
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.device)
+            self.max_mhz = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+            masks = {k: getattr(N, v) for k, v in self.REASONS.items()}
+
+            def run():
+                while not self._stop.is_set():
+                    self.sm.append(float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)))
+                    r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    for k, m in masks.items():
+                        if r & m:
+                            self.reasons.add(k)
+                    time.sleep(0.005)
+
+            self.t = threading.Thread(target=run, daemon=True)
             self.t.start()
-        except OSError:
-            self.proc = None
+        except Exception:
+            self.t = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
-
     def __exit__(self, *a):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self._stop.set()
+        if self.t is not None:
+            self.t.join(timeout=2)
 
     def summary(self):
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in self.rows:
-            for i, n in enumerate(names):
-                if len(r) > 5 + i and r[5 + i].lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+        if not self.sm:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(self.sm)), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.sm)}
 
 
 def make_problem():
@@ -181,7 +184,6 @@ def run_ours(args):
     L = lib()
     results = {}
     kernel_ms = {}
-    first_step = {}
     tuned = {}
     for prec in ("fp64", "fp32_bulk"):
         m.uold[:] = u0
@@ -200,7 +202,6 @@ def run_ours(args):
         m.uold[:] = u0
         gpu.push_uold()
         dt, _ = gpu.step_uniform()
-        first_step[prec] = gpu.fetch_uold()
         kernel_ms[prec] = kernel_time(gpu, args.steps, dt)
         if prec == "fp32_bulk":
             # end to end through the ABI with host buffers (pinned)
@@ -237,7 +238,10 @@ def run_ours(args):
             dist.barrier()
             dist.destroy_process_group()
         return
-    # one FP64 oracle step from the same state: CPU baseline + accuracy
+    # Accuracy on a developed blast (FP32-bulk vs FP64) and the CPU baseline:
+    # both GPU paths run ACC_STEPS steps from the initial state (cumulative
+    # error), then one step from the FP64 state is taken by the CPU oracle, the
+    # FP32-bulk path and the FP64 path (per-step error).
     cpu = None
     acc = None
     if not args.no_cpu:
@@ -245,19 +249,39 @@ def run_ours(args):
         import oracle
 
         nthreads = os.cpu_count() or 1
-        m.uold[:] = u0
+        states = {}
+        for prec in ("fp64", "fp32_bulk"):
+            m.uold[:] = u0
+            gpu = GodunovGPU(m, P, precision=prec, device=device)
+            for _ in range(args.acc_steps):
+                gpu.step_uniform()
+            states[prec] = gpu.fetch_uold()
+            gpu.close()
+        s_dev = states["fp64"]
+        m.uold[:] = s_dev
         o = oracle.OracleHydro(m, P, nthreads=nthreads)
         t0 = time.perf_counter()
         o.step_uniform()
         cpu_s = time.perf_counter() - t0
         ref = m.uold.copy()
+        one = {}
+        for prec in ("fp64", "fp32_bulk"):
+            m.uold[:] = s_dev
+            gpu = GodunovGPU(m, P, precision=prec, device=device)
+            gpu.step_uniform()
+            one[prec] = gpu.fetch_uold()
+            gpu.close()
+        names = ["rho", "mx", "my", "mz", "E"]
         cpu = {"value": ncell / cpu_s, "unit": "cell-updates/s", "cores": nthreads, "kind": "port",
-               "sample": "one full 256^3 Sedov step (courant_fine + godunov_fine, OpenMP over oct blocks) "
-                         "of the CPU restatement, %.2f s" % cpu_s}
-        acc = {"fp32_bulk_vs_fp64_oracle_rel_l1": dict(zip(["rho", "mx", "my", "mz", "E"],
-                                                           rel_l1(first_step["fp32_bulk"], ref))),
-               "fp64_vs_fp64_oracle_rel_l1": dict(zip(["rho", "mx", "my", "mz", "E"],
-                                                      rel_l1(first_step["fp64"], ref)))}
+               "sample": "one full 256^3 Sedov step (courant_fine + godunov_fine, OpenMP over oct blocks "
+                         "on %d threads) of the CPU restatement of the reference path, %.2f s" % (nthreads, cpu_s)}
+        acc = {"state": "Sedov3D 256^3 after %d FP64 steps" % args.acc_steps,
+               "per_step_fp32_bulk_vs_fp64_oracle_rel_l1": dict(zip(names, rel_l1(one["fp32_bulk"], ref))),
+               "per_step_fp64_vs_fp64_oracle_rel_l1": dict(zip(names, rel_l1(one["fp64"], ref))),
+               "cumulative_fp32_bulk_vs_fp64_rel_l1": dict(zip(names, rel_l1(states["fp32_bulk"], s_dev))),
+               "cumulative_steps": args.acc_steps}
+        acc["density_l1_le_1e-5"] = bool(acc["per_step_fp32_bulk_vs_fp64_oracle_rel_l1"]["rho"] <= 1e-5 and
+                                         acc["cumulative_fp32_bulk_vs_fp64_rel_l1"]["rho"] <= 1e-5)
     peak, peak_kind = measured_peaks()
     prec = "fp32_bulk"
     ms = results[prec]["ms_per_step"]
@@ -357,6 +381,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / accuracy leg")
+    ap.add_argument("--acc-steps", type=int, default=100, help="steps before the accuracy comparison")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
