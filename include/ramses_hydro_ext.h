@@ -37,6 +37,35 @@ int rh_bench_godunov(int ilevel, int nrep, double gamma, double smallr, double s
 int rh_timer_start(void);
 int rh_timer_stop(float* ms);
 
+/* ---- for callers that cannot allocate -------------------------------------
+ * rh_cmpdt_noalloc has no counterpart in the reference (RAMSES II's
+ * gpu_cmpdt_2 borrows scratch from a device array it owns).  It serves hosts
+ * that must not let a library call cudaMalloc/cudaFree: code capturing CUDA
+ * graphs, solvers whose own memory manager hands out all device memory under
+ * a fixed budget, and tight loops that cannot afford the device-wide
+ * synchronisation an allocation implies.
+ *
+ * courant_fine over a caller-owned FP64 state, allocating nothing:
+ * d_uold    device pointer to num_octs oct records in the reference layout
+ *           uold(1:8,1:5,1:num_octs) (320 bytes per oct);
+ * d_refined optional device pointer to num_octs*8 bytes, nonzero = refined
+ *           cell (skipped); NULL treats every cell as a leaf;
+ * d_out     device pointer to 5 doubles: mass, ekin (sum of E*vol, as the
+ *           reference names it), eint, emag (0), dt = min(dx/smallc, cell dt);
+ * stream    cudaStream_t to run on (NULL: the legacy default stream).
+ * Limit: num_octs <= 2,097,152 (one 256^3-cell level); larger sizes return
+ * RH_EINVAL without touching the GPU.  The per-block partials live in one
+ * file-scope device array of 2.6 MB that every GPU loading the library keeps
+ * until process exit; each block overwrites its own slot, so nothing needs
+ * clearing, and every call reuses the same array: calls that overlap on the
+ * GPU (different streams, or host threads sharing a device) race.  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * and caches it; make that first call before any stream capture.
+ * Asynchronous: read d_out after synchronising the stream. */
+int rh_cmpdt_noalloc(const double* d_uold, int num_octs, const unsigned char* d_refined, double dx,
+                     double gamma, double smallr, double smallc, double courant_factor,
+                     const double* constant_gravity, double* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
