@@ -54,20 +54,21 @@ static std::vector<RegEntry>& registry() {
 void register_launcher(const KernelKey& k, LaunchFn fn, size_t smem, int threads) {
   registry().push_back({k, fn, smem, threads});
 }
-LaunchFn find_launcher(int prec, int txo, int tyo, int minb, int slope, int riemann, size_t* smem, int* threads) {
+LaunchFn find_launcher(int prec, int txo, int tyo, int minb, int slope, int riemann, int amr, size_t* smem,
+                       int* threads) {
   for (auto& e : registry())
     if (e.k.prec == prec && e.k.txo == txo && e.k.tyo == tyo && e.k.minb == minb && e.k.slope == slope &&
-        e.k.riemann == riemann) {
+        e.k.riemann == riemann && e.k.amr == amr) {
       if (smem) *smem = e.smem;
       if (threads) *threads = e.threads;
       return e.fn;
     }
   return nullptr;
 }
-int list_tiles(int prec, int* txo, int* tyo, int* minb, int max) {
+int list_tiles(int prec, int amr, int* txo, int* tyo, int* minb, int max) {
   int n = 0;
   for (auto& e : registry()) {
-    if (e.k.prec != prec || e.k.slope != 2 || e.k.riemann != 3) continue;
+    if (e.k.prec != prec || e.k.slope != 2 || e.k.riemann != 3 || e.k.amr != amr) continue;
     if (n < max) {
       txo[n] = e.k.txo;
       tyo[n] = e.k.tyo;
@@ -215,6 +216,8 @@ static void free_tables(LevelTables& t) {
   cudaFree(t.d_poff);
   cudaFree(t.d_ptab);
   cudaFree(t.d_cfl_partial);
+  cudaFree(t.d_gsrc_oct);
+  cudaFree(t.d_gsrc_cf);
   t = LevelTables();
 }
 
@@ -230,6 +233,10 @@ static void free_state() {
   }
   cudaFree(c.d_cfl);
   cudaFree(c.d_scratch);
+  cudaFree(c.d_refmask);
+  cudaFree(c.d_gfather);
+  c.d_refmask = nullptr;
+  c.d_gfather = nullptr;
   c.d_cfl = nullptr;
   c.d_scratch = nullptr;
   c.scratch_elems = 0;
@@ -462,7 +469,7 @@ int rh_set_tile(int txo, int tyo, int minb, int lz) {
   int rc = check_ready(false);
   if (rc) return rc;
   Context& c = ctx();
-  if (!find_launcher(c.precision, txo, tyo, minb, 2, 3) || lz < 1) {
+  if (!find_launcher(c.precision, txo, tyo, minb, 2, 3, 0) || lz < 1) {
     set_error("tile %dx%d (minb=%d, lz=%d) is not compiled for this precision", txo, tyo, minb, lz);
     return RH_EINVAL;
   }
@@ -470,7 +477,7 @@ int rh_set_tile(int txo, int tyo, int minb, int lz) {
   c.cfg.tyo = tyo;
   c.cfg.minb = minb;
   c.cfg.lz = lz;
-  if (c.have_mesh)
+  if (c.have_mesh && c.nlevels_used == 1)
     for (int l = c.levelmin; l <= c.levelmax; ++l)
       if (c.levels[l].built) {
         rc = build_level_tables(l, c.cfg);
@@ -527,7 +534,26 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
     nused = std::max(nused, (long long)c.head[l] - 1 + c.noct[l]);
   }
   c.grid.assign(m->grid, m->grid + nused);
-  const long long n = c.ngridmax;
+  c.nlevels_used = 0;
+  for (int l = c.levelmin; l <= c.levelmax; ++l) c.nlevels_used += c.noct[l] > 0;
+  const bool multi = c.nlevels_used > 1;
+  c.levels.assign(c.levelmax + 1, LevelTables());
+  // coarse-fine levels: host tables first, they fix the number of ghost octs
+  long long nghost = 0;
+  for (int l = c.levelmin; l <= c.levelmax; ++l) {
+    if (c.noct[l] == 0) continue;
+    const long long box = ((long long)c.box_nx[0] << (l - 1)) * ((long long)c.box_nx[1] << (l - 1)) *
+                          ((long long)c.box_nx[2] << (l - 1));
+    if ((long long)c.noct[l] == box) continue;
+    rc = build_amr_tables(l, c.amr_cfg, (long long)c.ngridmax + nghost);
+    if (rc) {
+      c.levels.clear();
+      return rc;
+    }
+    nghost += c.levels[l].nghost;
+  }
+  c.nstate = (long long)c.ngridmax + nghost;
+  const long long n = c.nstate;
   for (int i = 0; i < 2; ++i) {
     if (c.precision == RH_PREC_FP64) {
       RH_CUDA(cudaMalloc(&c.ud[i], sizeof(double) * 40 * n));
@@ -537,9 +563,20 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
     }
   }
   RH_CUDA(cudaMalloc(&c.d_cfl, sizeof(double) * 5 * (c.levelmax + 1)));
+  {
+    std::vector<uint8_t> ref((size_t)n, 0);
+    for (long long i = 0; i < nused; ++i) {
+      uint8_t b = 0;
+      for (int k = 0; k < 8; ++k) b |= (uint8_t)((c.grid[i].refined[k] ? 1 : 0) << k);
+      ref[i] = b;
+    }
+    RH_CUDA(cudaMalloc(&c.d_refmask, (size_t)n));
+    RH_CUDA(cudaMemcpy(c.d_refmask, ref.data(), (size_t)n, cudaMemcpyHostToDevice));
+    RH_CUDA(cudaMalloc(&c.d_gfather, sizeof(int2) * (size_t)std::max(1LL, nghost)));
+  }
   c.cur = 0;
-  c.levels.assign(c.levelmax + 1, LevelTables());
   c.unew_pending.assign(c.levelmax + 1, 0);
+  c.unew_copied.assign(c.levelmax + 1, 0);
   c.unew_written.assign(c.levelmax + 1, 0);
   c.cfl_on_unew.assign(c.levelmax + 1, 0);
   c.cfl_on_uold.assign(c.levelmax + 1, 0);
@@ -548,7 +585,12 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
   if (rc) return rc;
   for (int l = c.levelmin; l <= c.levelmax; ++l) {
     if (c.noct[l] == 0) continue;
-    rc = build_level_tables(l, c.cfg);
+    if (c.levels[l].nghost > 0 || (c.levels[l].npencil > 0 && !c.levels[l].complete)) {
+      rc = upload_amr_tables(l);
+      if (rc) return rc;
+      continue;
+    }
+    rc = build_level_tables(l, multi ? c.amr_cfg : c.cfg);
     if (rc) {
       // keep the mesh usable for set_unew/set_uold/cmpdt; godunov on this
       // level will report the table error
@@ -620,14 +662,23 @@ int rh_set_unew(int head_idx, int num_octs) {
     return RH_EINVAL;
   }
   const int l = level_of_range(head_idx, num_octs);
-  if (l >= 0) {
+  if (l >= 0 && c.nlevels_used == 1) {
     // unew = uold is folded into the next rh_godunov of this level, which then
     // writes unew = uold + flux differences for every oct of the level.
     c.unew_pending[l] = 1;
     c.unew_written[l] = 0;
     return RH_OK;
   }
-  return copy_level(head_idx, num_octs, c.cur, 1 - c.cur);
+  // several levels: finer levels add coarse corrections into this unew before
+  // its own Godunov step, so the copy is made now (godunov_fine.f90:114-148)
+  int rc2 = copy_level(head_idx, num_octs, c.cur, 1 - c.cur);
+  if (rc2) return rc2;
+  if (l >= 0) {
+    c.unew_copied[l] = 1;
+    c.unew_pending[l] = 0;
+    c.unew_written[l] = 0;
+  }
+  return RH_OK;
 }
 
 int rh_set_uold(int head_idx, int num_octs) {
@@ -661,6 +712,7 @@ int rh_set_uold(int head_idx, int num_octs) {
   if (rc) return rc;
   if (l >= 0) {
     c.unew_written[l] = 0;
+    c.unew_copied[l] = 0;
     c.cfl_on_uold[l] = c.cfl_on_unew[l];
     c.cfl_on_unew[l] = 0;
   }
@@ -746,21 +798,31 @@ int rh_cmpdt(int head_idx, int num_octs, double dx, double gamma, double smallr,
 // Launch one Godunov step of level l with the given tile configuration.
 // Exposed to the batch/bench layer through rh_godunov and rh_bench_*.
 static int launch_level(int l, double gamma, double smallr, double smallc, double dt, double dx, double smax_cap,
-                        int slope, int riemann, const double* g, bool fuse_cfl) {
+                        int slope, int riemann, const double* g, bool fuse_cfl, bool accumulate = false) {
   Context& c = ctx();
   LevelTables& T = c.levels[l];
-  if (!T.built || T.cfg.txo != c.cfg.txo || T.cfg.tyo != c.cfg.tyo || T.cfg.lz != c.cfg.lz) {
-    int rc = build_level_tables(l, c.cfg);
-    if (rc) return rc;
+  const bool amr = c.nlevels_used > 1;  // refined cells / coarse-fine faces exist on every level
+  const TileCfg& want = amr ? c.amr_cfg : c.cfg;
+  if (T.complete || !T.built) {
+    if (!T.built || T.cfg.txo != want.txo || T.cfg.tyo != want.tyo || T.cfg.lz != want.lz) {
+      int rc = build_level_tables(l, want);
+      if (rc) return rc;
+    }
   }
   size_t smem = 0;
   int threads = 0;
-  LaunchFn fn = find_launcher(c.precision, T.cfg.txo, T.cfg.tyo, c.cfg.minb, slope, riemann, &smem, &threads);
+  LaunchFn fn = find_launcher(c.precision, T.cfg.txo, T.cfg.tyo, want.minb, slope, riemann, amr ? 1 : 0, &smem,
+                              &threads);
   if (!fn) {
-    set_error("no kernel for precision %d tile %dx%d (minb %d) slope %d riemann %d", c.precision, T.cfg.txo,
-              T.cfg.tyo, c.cfg.minb, slope, riemann);
+    set_error("no kernel for precision %d tile %dx%d (minb %d) slope %d riemann %d amr %d", c.precision, T.cfg.txo,
+              T.cfg.tyo, want.minb, slope, riemann, amr ? 1 : 0);
     return RH_EINVAL;
   }
+  if (amr) {
+    int rc = prolong_ghosts(l, smallr);
+    if (rc) return rc;
+  }
+  if (T.npencil == 0) return RH_OK;
   LevelArgs A;
   A.phdr = T.d_phdr;
   A.poff = T.d_poff;
@@ -777,6 +839,9 @@ static int launch_level(int l, double gamma, double smallr, double smallc, doubl
   A.cfl = make_cfl(dx, gamma, smallr, smallc, courant, g);
   A.vol = dx * dx * dx;
   A.cfl_partial = fuse_cfl ? T.d_cfl_partial : nullptr;
+  A.refmask = c.d_refmask;
+  A.ghost_father = c.d_gfather;
+  A.accumulate = accumulate ? 1 : 0;
   const int nxt = 1 - c.cur;
   A.gm1_d = gamma - 1.0;
   A.smalle_d = smallc * smallc / gamma / (gamma - 1.0);
@@ -842,7 +907,7 @@ int rh_godunov(int head_idx, int num_subgrids, int ngridmax, int ilevel, int lev
     set_error("rh_godunov: riemann %d not supported (llf=1, hll=2, hllc=3)", riemann);
     return RH_EINVAL;
   }
-  if (!c.unew_pending[l]) {
+  if (!c.unew_pending[l] && !c.unew_copied[l]) {
     set_error("rh_godunov: call rh_set_unew for level %d first (unew must start as uold)", l);
     return RH_ESTATE;
   }
@@ -853,7 +918,8 @@ int rh_godunov(int head_idx, int num_subgrids, int ngridmax, int ilevel, int lev
   const bool fuse = c.cfl_key[0] == dx && c.cfl_key[1] == gamma && c.cfl_key[2] == smallr &&
                     c.cfl_key[5] == g[0] && c.cfl_key[6] == g[1] && c.cfl_key[7] == g[2] &&
                     c.cfl_key[3] * c.cfl_key[3] == smallc2;
-  rc = launch_level(l, gamma, smallr, std::sqrt(smallc2), dt, dx, smax_cap, slope, riemann, g, fuse);
+  rc = launch_level(l, gamma, smallr, std::sqrt(smallc2), dt, dx, smax_cap, slope, riemann, g, fuse,
+                    c.unew_copied[l] != 0);
   if (rc) return rc;
   c.unew_pending[l] = 0;
   c.unew_written[l] = 1;
@@ -932,7 +998,7 @@ int rh_get_tile(int* txo, int* tyo, int* minb, int* lz) {
 }
 
 int rh_list_tiles(int precision, int* txo, int* tyo, int* minb, int max) {
-  return list_tiles(precision, txo, tyo, minb, max);
+  return list_tiles(precision, 0, txo, tyo, minb, max);
 }
 
 int rh_level_info(int ilevel, int* npencil, long long* table_entries) {

@@ -70,6 +70,7 @@ template <typename T, typename V, int TXO, int TYO> struct Geo {
   static constexpr size_t kFS = (size_t)10 * NRC * sizeof(V);
   static constexpr size_t kFX = (size_t)2 * 5 * NRC * sizeof(V);
   static constexpr size_t kRed = (size_t)NWARP * 4 * sizeof(double);
+  static constexpr size_t kAmr = (size_t)NRC * (sizeof(int) + sizeof(uint32_t));
   static constexpr size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
   static constexpr size_t oStageD = 0;
   static constexpr size_t oStageF = a16(oStageD + kStageD);
@@ -77,7 +78,8 @@ template <typename T, typename V, int TXO, int TYO> struct Geo {
   static constexpr size_t oFS = a16(oQ + kQ);
   static constexpr size_t oFX = a16(oFS + kFS);
   static constexpr size_t oRed = a16(oFX + kFX);
-  static constexpr size_t oBar = a16(oRed + kRed);
+  static constexpr size_t oAmr = a16(oRed + kRed);
+  static constexpr size_t oBar = a16(oAmr + kAmr);
   static constexpr size_t kSmem = oBar + 64;
 };
 
@@ -116,7 +118,45 @@ struct LevelArgs {
   CflConst cfl;
   double vol;
   double gm1_d, smalle_d;  // FP64 pressure recovery constants
+  // coarse-fine levels only
+  const uint8_t* refmask;  // per oct (real and ghost): bit c = cell c refined
+  const int2* ghost_father;  // per ghost (entry - ghost_base): father oct (0-based), father cell
+  int accumulate;          // 1: unew already holds uold (+ finer-level corrections); add to it
 };
+
+// Coarse-fine status of one cell of an AMR level (hydro/godunov_fine.f90:
+// 666-685 flux reset, 893-1052 coarse update): bit 0 refined, bit 1 a cell of
+// this level updated by this pencil, bit 2 an interpolated ghost inside the
+// domain (its father cell receives the face flux / 8).
+__device__ __forceinline__ uint32_t amr_bits(const LevelArgs& A, int ent, int cell, bool upd_pos, bool in_dom) {
+  uint32_t b = 0;
+  if (ent >= 0) {
+    b = (A.refmask[ent] >> cell) & 1u;
+    if (ent < A.ghost_base) b |= upd_pos ? 2u : 0u;
+    else b |= in_dom ? 4u : 0u;
+  }
+  return b;
+}
+
+// Flux through the face between a cell of this level and an interpolated
+// ghost: unew(father) +- flux/8 (sign -1: ghost on the low side).
+__device__ __forceinline__ void coarse_add_f64(const LevelArgs& A, double* unew, int ghost_ent, const double* f,
+                                               double sign) {
+  const int2 fa = A.ghost_father[ghost_ent - A.ghost_base];
+  if (fa.x < 0) return;
+  double* o = unew + (size_t)fa.x * 40 + fa.y;
+#pragma unroll
+  for (int n = 0; n < 5; ++n) atomicAdd(o + 8 * n, sign * (f[n] * 0.125));
+}
+__device__ __forceinline__ void coarse_add_f32(const LevelArgs& A, float* unew_f, double* unew_e, int ghost_ent,
+                                               const float* f, float sign) {
+  const int2 fa = A.ghost_father[ghost_ent - A.ghost_base];
+  if (fa.x < 0) return;
+  float* o = unew_f + (size_t)fa.x * 32 + fa.y;
+#pragma unroll
+  for (int n = 0; n < 4; ++n) atomicAdd(o + 8 * n, sign * (f[n] * 0.125f));
+  atomicAdd(unew_e + (size_t)fa.x * 8 + fa.y, (double)sign * ((double)f[4] * 0.125));
+}
 
 template <typename T> struct StateArgs {
   const double* uold_d;  // FP64 [oct][5][8]  or FP32-bulk energy [oct][8]
@@ -178,7 +218,7 @@ template <int NWARP> __device__ __forceinline__ void cfl_block_reduce(const CflA
 template <class G> struct Columns {
   int rx, ry, lc, slot;
   CellMap mx, my;
-  bool interior, in_domain_xy, has_outer;
+  bool interior, in_domain_xy, in_dom_xy, has_outer;
   int orx, ory, olc, oslot;
   CellMap omx, omy;
   static constexpr int kStride = G::NT / G::NOC > 0 ? G::NT / G::NOC : 1;
@@ -192,6 +232,7 @@ template <class G> struct Columns {
     slot = ((rx >> 1) + 1) + G::OW * ((ry >> 1) + 1);
     interior = rx >= 0 && rx < G::CX && ry >= 0 && ry < G::CY;
     in_domain_xy = gx < A.ncx && gy < A.ncy;
+    in_dom_xy = gx >= 0 && gy >= 0 && in_domain_xy;
     int o = (t % kStride == 0) ? t / kStride : -1;
     if (o >= G::NOC) o = -1;
     has_outer = o >= 0;
@@ -291,7 +332,7 @@ __device__ __forceinline__ void ctoprim_f64(const double* sd, int cell, bool fx,
   q[4] = H.gm1 * eint;
 }
 
-template <typename T, int TXO, int TYO, int MINB, int SLOPE, int RIEMANN>
+template <typename T, int TXO, int TYO, int MINB, int SLOPE, int RIEMANN, bool AMR>
 __global__ void __launch_bounds__(Geo<T, double, TXO, TYO>::NT, MINB)
 godunov_pencil_kernel(const LevelArgs A, const StateArgs<T> S, const HydroK<double> H) {
   using G = Geo<T, double, TXO, TYO>;
@@ -300,6 +341,8 @@ godunov_pencil_kernel(const LevelArgs A, const StateArgs<T> S, const HydroK<doub
   double* FS = reinterpret_cast<double*>(smem + G::oFS);   // [10][NRC]: qp_x(5), qp_y(5)
   double* FXY = reinterpret_cast<double*>(smem + G::oFX);  // [2][5][NRC]: x then y fluxes
   double* red = reinterpret_cast<double*>(smem + G::oRed);
+  int* entb = reinterpret_cast<int*>(smem + G::oAmr);                    // AMR: entry of plane k
+  uint32_t* stb = reinterpret_cast<uint32_t*>(smem + G::oAmr + G::NRC * sizeof(int));  // AMR: status bits
   __shared__ int s_abort;
 
   const int t = threadIdx.x;
@@ -341,10 +384,22 @@ godunov_pencil_kernel(const LevelArgs A, const StateArgs<T> S, const HydroK<doub
       for (int n = 0; n < 5; ++n) Qp[n * G::NLC + col.olc] = qo[n];
     }
   };
+  // AMR: table entry and status bits of the own cell at plane p
+  auto status = [&](int p, int& ent) -> uint32_t {
+    const int row = (p >> 1) + 1;
+    const CellMap mz = zmap(p);
+    ent = tab[(long long)row * G::NSLOT + col.slot];
+    const int gz = 2 * oz0 + p;
+    const bool in_dom = col.in_dom_xy && gz >= 0 && gz < A.ncz;
+    const bool upd = col.interior && in_dom && p >= 0 && p < CZ;
+    return amr_bits(A, ent, col.mx.parity + 2 * col.my.parity + 4 * mz.parity, upd, in_dom);
+  };
 
   double qa[5], qb[5], qc[5], irb = 0, irc = 0;  // own column, planes k-1, k, k+1
   double Uk[5], Uk1[5];                          // uold of planes k, k+1
   double qmx[5], qmy[5], qmz_prev[5], fz_prev[5], up[5];
+  int ea = -1, eb = -1, ec = -1;                 // AMR: entries of planes k-1, k, k+1
+  uint32_t sa = 0, sb = 0, sc = 0;               // AMR: status bits of planes k-1, k, k+1
   CflAcc acc;
 #pragma unroll
   for (int n = 0; n < 5; ++n) { qmz_prev[n] = 0; fz_prev[n] = 0; up[n] = 0; Uk[n] = 0; Uk1[n] = 0; qc[n] = 0; }
@@ -356,6 +411,7 @@ godunov_pencil_kernel(const LevelArgs A, const StateArgs<T> S, const HydroK<doub
     convert(-2, qa, ira, Uk1, false);
   }
   convert(-1, qb, irb, Uk1, true);
+  if (AMR && active) sb = status(-1, eb);
   __syncthreads();
   if (L + 1 >= 2) stg.issue(2);
 
@@ -365,6 +421,7 @@ godunov_pencil_kernel(const LevelArgs A, const StateArgs<T> S, const HydroK<doub
       const int p = k + 1;
       if ((p & 1) == 0) stg.wait((p >> 1) + 1);
       convert(p, qc, irc, Uk1, true);
+      if (AMR && active) sc = status(p, ec);
     }
     // (C) slopes, predictor and interface states of plane k
     double fz[5] = {0, 0, 0, 0, 0};
@@ -403,6 +460,10 @@ godunov_pencil_kernel(const LevelArgs A, const StateArgs<T> S, const HydroK<doub
         qmx[n] = qm[0][n];
         qmy[n] = qm[1][n];
       }
+      if (AMR) {
+        entb[t] = eb;
+        stb[t] = sb;
+      }
       // z interface k-1/2: left = qm_z(k-1), right = qp_z(k); rotation (r,w,u,v,p)
       if (col.interior && k >= 0) {
         const double ql[5] = {qmz_prev[0], qmz_prev[3], qmz_prev[1], qmz_prev[2], qmz_prev[4]};
@@ -410,6 +471,14 @@ godunov_pencil_kernel(const LevelArgs A, const StateArgs<T> S, const HydroK<doub
         double f[5];
         riemann_dtdx<double, RIEMANN>(ql, qr, f, H);
         fz[0] = f[0]; fz[3] = f[1]; fz[1] = f[2]; fz[2] = f[3]; fz[4] = f[4];
+        if (AMR) {
+          if ((sa | sb) & 1u) {
+#pragma unroll
+            for (int n = 0; n < 5; ++n) fz[n] = 0.0;
+          }
+          if ((sa & 2u) && (sb & 4u)) coarse_add_f64(A, S.unew_d, eb, fz, 1.0);
+          if ((sa & 4u) && (sb & 2u)) coarse_add_f64(A, S.unew_d, ea, fz, -1.0);
+        }
       }
 #pragma unroll
       for (int n = 0; n < 5; ++n) qmz_prev[n] = qm[2][n];
@@ -424,6 +493,15 @@ godunov_pencil_kernel(const LevelArgs A, const StateArgs<T> S, const HydroK<doub
                               FS[3 * G::NRC + t + 1], FS[4 * G::NRC + t + 1]};
         double f[5];
         riemann_dtdx<double, RIEMANN>(qmx, qr, f, H);
+        if (AMR) {
+          const uint32_t bl = stb[t], br = stb[t + 1];
+          if ((bl | br) & 1u) {
+#pragma unroll
+            for (int n = 0; n < 5; ++n) f[n] = 0.0;
+          }
+          if ((bl & 2u) && (br & 4u)) coarse_add_f64(A, S.unew_d, entb[t + 1], f, 1.0);
+          if ((bl & 4u) && (br & 2u)) coarse_add_f64(A, S.unew_d, entb[t], f, -1.0);
+        }
 #pragma unroll
         for (int n = 0; n < 5; ++n) FXY[n * G::NRC + t] = f[n];
       }
@@ -434,12 +512,19 @@ godunov_pencil_kernel(const LevelArgs A, const StateArgs<T> S, const HydroK<doub
                               FS[9 * G::NRC + tn]};
         double f[5];
         riemann_dtdx<double, RIEMANN>(ql, qr, f, H);
+        double fy[5] = {f[0], f[2], f[1], f[3], f[4]};
+        if (AMR) {
+          const uint32_t bl = stb[t], br = stb[tn];
+          if ((bl | br) & 1u) {
+#pragma unroll
+            for (int n = 0; n < 5; ++n) fy[n] = 0.0;
+          }
+          if ((bl & 2u) && (br & 4u)) coarse_add_f64(A, S.unew_d, entb[tn], fy, 1.0);
+          if ((bl & 4u) && (br & 2u)) coarse_add_f64(A, S.unew_d, entb[t], fy, -1.0);
+        }
         double* FY = FXY + 5 * G::NRC;
-        FY[0 * G::NRC + t] = f[0];
-        FY[2 * G::NRC + t] = f[1];
-        FY[1 * G::NRC + t] = f[2];
-        FY[3 * G::NRC + t] = f[3];
-        FY[4 * G::NRC + t] = f[4];
+#pragma unroll
+        for (int n = 0; n < 5; ++n) FY[n * G::NRC + t] = fy[n];
       }
     }
     __syncthreads();  // S3: fluxes of plane k published
@@ -456,15 +541,28 @@ godunov_pencil_kernel(const LevelArgs A, const StateArgs<T> S, const HydroK<doub
           for (int n = 0; n < 5; ++n) un[n] = up[n] + (fz_prev[n] - fz[n]);
           double* o = S.unew_d + (size_t)oct * 40 + cell;
           o[0] = un[0]; o[8] = un[1]; o[16] = un[2]; o[24] = un[3]; o[32] = un[4];
-          if (A.cfl_partial) acc.add(un[0], un[1], un[2], un[3], un[4], A);
+          if (A.cfl_partial && !(AMR && (sa & 1u))) acc.add(un[0], un[1], un[2], un[3], un[4], A);
         }
       }
       if (plane_ok) {
         const double* FX = FXY;
         const double* FY = FXY + 5 * G::NRC;
+        double base[5];
+#pragma unroll
+        for (int n = 0; n < 5; ++n) base[n] = Uk[n];
+        if (AMR && A.accumulate) {
+          // unew holds uold plus the finer level's coarse corrections
+          const int oct = tab[(long long)((k >> 1) + 1) * G::NSLOT + col.slot];
+          if (col.in_domain_xy && 2 * oz0 + k < A.ncz && oct >= 0 && oct < A.ghost_base) {
+            const int cell = (col.rx & 1) + 2 * (col.ry & 1) + 4 * (k & 1);
+            const double* o = S.unew_d + (size_t)oct * 40 + cell;
+#pragma unroll
+            for (int n = 0; n < 5; ++n) base[n] = o[8 * n];
+          }
+        }
 #pragma unroll
         for (int n = 0; n < 5; ++n) {
-          const double u0 = Uk[n] + (FX[n * G::NRC + t - 1] - FX[n * G::NRC + t]);
+          const double u0 = base[n] + (FX[n * G::NRC + t - 1] - FX[n * G::NRC + t]);
           up[n] = u0 + (FY[n * G::NRC + t - G::RW] - FY[n * G::NRC + t]);
         }
       }
@@ -472,6 +570,8 @@ godunov_pencil_kernel(const LevelArgs A, const StateArgs<T> S, const HydroK<doub
 #pragma unroll
     for (int n = 0; n < 5; ++n) { fz_prev[n] = fz[n]; Uk[n] = Uk1[n]; qa[n] = qb[n]; qb[n] = qc[n]; }
     irb = irc;
+    ea = eb; eb = ec;
+    sa = sb; sb = sc;
   }
   if (A.cfl_partial) cfl_block_reduce<G::NWARP>(acc, red, A.cfl_partial + (size_t)pencil * 5);
 }

@@ -50,7 +50,32 @@ __device__ __forceinline__ void ctoprim_f32x2(const float* sf, const double* sd,
   q[4] = make_float2((float)(gm1 * e0), (float)(gm1 * e1));
 }
 
-template <int TXO, int TYO, int MINB, int SLOPE, int RIEMANN>
+// Flux reset and coarse corrections of one x or y face of a layer, per plane
+// (.x plane 2K, .y plane 2K+1); bl/br: status bits (a | b<<8) of the cells
+// left/right of the face, el/er their oct entries.
+__device__ __forceinline__ void amr_face_f32(const LevelArgs& A, const StateArgs<float>& S, float2* f, uint32_t bl,
+                                             uint32_t br, int el, int er) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t l = (bl >> (8 * h)) & 0xffu, r = (br >> (8 * h)) & 0xffu;
+    float c[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) c[n] = h ? f[n].y : f[n].x;
+    if ((l | r) & 1u) {
+#pragma unroll
+      for (int n = 0; n < 5; ++n) c[n] = 0.f;
+    }
+    if ((l & 2u) && (r & 4u)) coarse_add_f32(A, S.unew_f, S.unew_d, er, c, 1.f);
+    if ((l & 4u) && (r & 2u)) coarse_add_f32(A, S.unew_f, S.unew_d, el, c, -1.f);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      if (h) f[n].y = c[n];
+      else f[n].x = c[n];
+    }
+  }
+}
+
+template <int TXO, int TYO, int MINB, int SLOPE, int RIEMANN, bool AMR>
 __global__ void __launch_bounds__(Geo<float, float2, TXO, TYO>::NT, MINB)
 godunov_pencil2_kernel(const LevelArgs A, const StateArgs<float> S, const HydroK<float2> H) {
   using G = Geo<float, float2, TXO, TYO>;
@@ -59,6 +84,8 @@ godunov_pencil2_kernel(const LevelArgs A, const StateArgs<float> S, const HydroK
   float2* FS = reinterpret_cast<float2*>(smem + G::oFS);   // [10][NRC]
   float2* FXY = reinterpret_cast<float2*>(smem + G::oFX);  // [2][5][NRC]
   double* red = reinterpret_cast<double*>(smem + G::oRed);
+  int* entb = reinterpret_cast<int*>(smem + G::oAmr);                                   // AMR: entry of layer K
+  uint32_t* stb = reinterpret_cast<uint32_t*>(smem + G::oAmr + G::NRC * sizeof(int));  // AMR: bits a | b<<8
   __shared__ int s_abort;
 
   const int t = threadIdx.x;
@@ -103,6 +130,22 @@ godunov_pencil2_kernel(const LevelArgs A, const StateArgs<float> S, const HydroK
     }
     (void)ocxy;
   };
+  // AMR: entry of layer K and status bits of its two planes (a | b << 8)
+  auto status = [&](int K, int& ent) -> uint32_t {
+    const int row = K + 1;
+    ent = tab[(long long)row * G::NSLOT + col.slot];
+    uint32_t bits = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int p = 2 * K + h;
+      const CellMap mz = map_coord(2 * oz0 + p, A.ncz, A.periodic[2], A.btype[4], A.btype[5]);
+      const int gz = 2 * oz0 + p;
+      const bool in_dom = col.in_dom_xy && gz >= 0 && gz < A.ncz;
+      const bool upd = col.interior && in_dom && K >= 0 && K < L;
+      bits |= amr_bits(A, ent, col.mx.parity + 2 * col.my.parity + 4 * mz.parity, upd, in_dom) << (8 * h);
+    }
+    return bits;
+  };
 
   float2 cur[5], nxt[5], irc, irn;
   float prv_b[5];
@@ -113,6 +156,9 @@ godunov_pencil2_kernel(const LevelArgs A, const StateArgs<float> S, const HydroK
   float upb[4], fzb[5];           // pending plane 2K-1: x/y-updated bulk values, flux at face 2K-1/2
   double upbE = 0;
   int pend_oct = -1;
+  bool pend_ref = false;
+  int ec = -1, en = -1, ep = -1;       // AMR: entries of layers K, K+1, K-1
+  uint32_t sc = 0, sn = 0, sp = 0;     // AMR: status bits of layers K, K+1, K-1
   CflAcc acc;
 #pragma unroll
   for (int n = 0; n < 5; ++n) { qmz_b[n] = 0.f; fzb[n] = 0.f; }
@@ -123,6 +169,7 @@ godunov_pencil2_kernel(const LevelArgs A, const StateArgs<float> S, const HydroK
   // prologue: layer -1 (table row 0)
   stg.wait(0);
   convert(-1, cur, irc, Uc, Ec);
+  if (AMR && active) sc = status(-1, ec);
 #pragma unroll
   for (int n = 0; n < 5; ++n) prv_b[n] = cur[n].x;  // plane -3 is never used
   __syncthreads();
@@ -133,6 +180,7 @@ godunov_pencil2_kernel(const LevelArgs A, const StateArgs<float> S, const HydroK
     if (K + 1 <= L) {
       stg.wait(K + 2);
       convert(K + 1, nxt, irn, Un, En);
+      if (AMR && active) sn = status(K + 1, en);
     } else {
 #pragma unroll
       for (int n = 0; n < 5; ++n) nxt[n] = cur[n];  // plane 2L+2 only feeds the unused plane 2L+1
@@ -190,6 +238,28 @@ godunov_pencil2_kernel(const LevelArgs A, const StateArgs<float> S, const HydroK
         }
         riemann_dtdx<float2, RIEMANN>(ql, qr, f, H);
         fz[0] = f[0]; fz[3] = f[1]; fz[1] = f[2]; fz[2] = f[3]; fz[4] = f[4];
+        if (AMR) {
+          // face .x: plane 2K-1 (layer K-1, plane b) / plane 2K (layer K, plane a);
+          // face .y: the two planes of layer K (one oct: never coarse-fine)
+          const uint32_t lo = sp >> 8, a = sc & 0xffu, b = sc >> 8;
+          if ((lo | a) & 1u) {
+#pragma unroll
+            for (int n = 0; n < 5; ++n) fz[n].x = 0.f;
+          }
+          if ((a | b) & 1u) {
+#pragma unroll
+            for (int n = 0; n < 5; ++n) fz[n].y = 0.f;
+          }
+          float fx_[5];
+#pragma unroll
+          for (int n = 0; n < 5; ++n) fx_[n] = fz[n].x;
+          if ((lo & 2u) && (a & 4u)) coarse_add_f32(A, S.unew_f, S.unew_d, ec, fx_, 1.f);
+          if ((lo & 4u) && (a & 2u)) coarse_add_f32(A, S.unew_f, S.unew_d, ep, fx_, -1.f);
+        }
+      }
+      if (AMR) {
+        entb[t] = ec;
+        stb[t] = sc;
       }
 #pragma unroll
       for (int n = 0; n < 5; ++n) qmz_b[n] = qm[2][n].y;
@@ -204,6 +274,7 @@ godunov_pencil2_kernel(const LevelArgs A, const StateArgs<float> S, const HydroK
 #pragma unroll
         for (int n = 0; n < 5; ++n) qr[n] = FS[n * G::NRC + t + 1];
         riemann_dtdx<float2, RIEMANN>(qmx, qr, f, H);
+        if (AMR) amr_face_f32(A, S, f, stb[t], stb[t + 1], entb[t], entb[t + 1]);
 #pragma unroll
         for (int n = 0; n < 5; ++n) FXY[n * G::NRC + t] = f[n];
       }
@@ -214,12 +285,11 @@ godunov_pencil2_kernel(const LevelArgs A, const StateArgs<float> S, const HydroK
                               FS[9 * G::NRC + tn]};
         float2 f[5];
         riemann_dtdx<float2, RIEMANN>(ql, qr, f, H);
+        float2 fy[5] = {f[0], f[2], f[1], f[3], f[4]};
+        if (AMR) amr_face_f32(A, S, fy, stb[t], stb[tn], entb[t], entb[tn]);
         float2* FY = FXY + 5 * G::NRC;
-        FY[0 * G::NRC + t] = f[0];
-        FY[2 * G::NRC + t] = f[1];
-        FY[1 * G::NRC + t] = f[2];
-        FY[3 * G::NRC + t] = f[3];
-        FY[4 * G::NRC + t] = f[4];
+#pragma unroll
+        for (int n = 0; n < 5; ++n) FY[n * G::NRC + t] = fy[n];
       }
     }
     __syncthreads();  // S3: fluxes of layer K published
@@ -233,25 +303,37 @@ godunov_pencil2_kernel(const LevelArgs A, const StateArgs<float> S, const HydroK
         const double Eb = upbE + (double)(fzb[4] - fz[4].x);
         o[0] = ub[0]; o[8] = ub[1]; o[16] = ub[2]; o[24] = ub[3];
         S.unew_d[(size_t)pend_oct * 8 + cxy + 4] = Eb;
-        if (A.cfl_partial) acc.add(ub[0], ub[1], ub[2], ub[3], Eb, A);
+        if (A.cfl_partial && !pend_ref) acc.add(ub[0], ub[1], ub[2], ub[3], Eb, A);
         pend_oct = -1;
       }
       if (layer_ok) {
         const float2* FX = FXY;
         const float2* FY = FXY + 5 * G::NRC;
+        const int gz = 2 * oz0 + 2 * K;
+        const int oct = tab[(long long)(K + 1) * G::NSLOT + col.slot];
+        const bool ok = col.in_domain_xy && gz < A.ncz && oct >= 0 && oct < A.ghost_base;
+        float2 base[4];
+        double Eba[2] = {Ec[0], Ec[1]};
+#pragma unroll
+        for (int n = 0; n < 4; ++n) base[n] = Uc[n];
+        if (AMR && A.accumulate && ok) {
+          // unew holds uold plus the finer level's coarse corrections
+          const float* o = S.unew_f + (size_t)oct * 32 + cxy;
+#pragma unroll
+          for (int n = 0; n < 4; ++n) base[n] = make_float2(o[8 * n], o[8 * n + 4]);
+          Eba[0] = S.unew_d[(size_t)oct * 8 + cxy];
+          Eba[1] = S.unew_d[(size_t)oct * 8 + cxy + 4];
+        }
         // reference order per cell: ((u + dFx) + dFy) + dFz
         float2 u2[4];
 #pragma unroll
         for (int n = 0; n < 4; ++n)
-          u2[n] = (Uc[n] + (FX[n * G::NRC + t - 1] - FX[n * G::NRC + t])) +
+          u2[n] = (base[n] + (FX[n * G::NRC + t - 1] - FX[n * G::NRC + t])) +
                   (FY[n * G::NRC + t - G::RW] - FY[n * G::NRC + t]);
-        const double ea = (Ec[0] + (double)(FX[4 * G::NRC + t - 1].x - FX[4 * G::NRC + t].x)) +
+        const double ea = (Eba[0] + (double)(FX[4 * G::NRC + t - 1].x - FX[4 * G::NRC + t].x)) +
                           (double)(FY[4 * G::NRC + t - G::RW].x - FY[4 * G::NRC + t].x);
-        const double eb = (Ec[1] + (double)(FX[4 * G::NRC + t - 1].y - FX[4 * G::NRC + t].y)) +
+        const double eb = (Eba[1] + (double)(FX[4 * G::NRC + t - 1].y - FX[4 * G::NRC + t].y)) +
                           (double)(FY[4 * G::NRC + t - G::RW].y - FY[4 * G::NRC + t].y);
-        const int gz = 2 * oz0 + 2 * K;
-        const int oct = tab[(long long)(K + 1) * G::NSLOT + col.slot];
-        const bool ok = col.in_domain_xy && gz < A.ncz && oct >= 0 && oct < A.ghost_base;
         if (ok) {
           float ua[4];
 #pragma unroll
@@ -260,12 +342,13 @@ godunov_pencil2_kernel(const LevelArgs A, const StateArgs<float> S, const HydroK
           float* o = S.unew_f + (size_t)oct * 32 + cxy;
           o[0] = ua[0]; o[8] = ua[1]; o[16] = ua[2]; o[24] = ua[3];
           S.unew_d[(size_t)oct * 8 + cxy] = Ea;
-          if (A.cfl_partial) acc.add(ua[0], ua[1], ua[2], ua[3], Ea, A);
+          if (A.cfl_partial && !(AMR && (sc & 1u))) acc.add(ua[0], ua[1], ua[2], ua[3], Ea, A);
 #pragma unroll
           for (int n = 0; n < 4; ++n) { upb[n] = u2[n].y; fzb[n] = fz[n].y; }
           fzb[4] = fz[4].y;
           upbE = eb;
           pend_oct = (gz + 1 < A.ncz) ? oct : -1;
+          pend_ref = AMR && ((sc >> 8) & 1u);
         }
       }
     }
@@ -276,6 +359,8 @@ godunov_pencil2_kernel(const LevelArgs A, const StateArgs<float> S, const HydroK
     Ec[0] = En[0];
     Ec[1] = En[1];
     irc = irn;
+    ep = ec; ec = en;
+    sp = sc; sc = sn;
   }
   if (A.cfl_partial) cfl_block_reduce<G::NWARP>(acc, red, A.cfl_partial + (size_t)pencil * 5);
 }

@@ -1,0 +1,6 @@
+// Coarse-fine (AMR) pencil-kernel instantiations: float bulk storage,
+// 8x4-oct XY tiles, registers sized for 2 CTAs per SM.
+#include "rh_launch.h"
+namespace rh {
+static TileRegistrar<float, 8, 4, 2, true> reg_amr_f32_8x4_b2;
+}

@@ -1,0 +1,6 @@
+// Coarse-fine (AMR) pencil-kernel instantiations: double bulk storage,
+// 4x4-oct XY tiles, registers sized for 2 CTAs per SM.
+#include "rh_launch.h"
+namespace rh {
+static TileRegistrar<double, 4, 4, 2, true> reg_amr_f64_4x4_b2;
+}

@@ -30,6 +30,15 @@ struct TileCfg {
 struct LevelTables {
   bool built = false;
   bool complete = false;  // level covers its whole box (uniform level)
+  // coarse-fine levels: interpolated ghost octs [gbase, gbase + nghost) of the
+  // state arrays, prolonged from level l-1 before each Godunov step
+  long long gbase = 0;
+  int nghost = 0;
+  std::vector<int> gsrc_oct;         // [nghost][7] level l-1 oct (0-based) of the 7 father-neighbourhood cells
+  std::vector<unsigned char> gsrc_cf;  // [nghost][7] cell | flip bits (x,y,z momentum) << 3
+  std::vector<int2> gfather;         // [nghost] father oct (0-based), father cell
+  int* d_gsrc_oct = nullptr;
+  unsigned char* d_gsrc_cf = nullptr;
   int nxo = 0, nyo = 0, nzo = 0;
   TileCfg cfg;
   int npencil = 0;
@@ -44,6 +53,7 @@ struct LevelTables {
 
 struct Context {
   bool inited = false;
+  TileCfg amr_cfg{4, 4, 2, 8};  // tiles of coarse-fine levels
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
@@ -65,12 +75,17 @@ struct Context {
   int cur = 0;
   double* ud[2] = {nullptr, nullptr};
   float* uf[2] = {nullptr, nullptr};
+  long long nstate = 0;            // ngridmax + interpolated ghost octs of all levels
+  uint8_t* d_refmask = nullptr;    // [nstate] refined-cell bits (ghosts: 0)
+  int2* d_gfather = nullptr;       // [nstate - ngridmax] father of each ghost
+  int nlevels_used = 0;
   int* d_err = nullptr;
   double* d_cfl = nullptr;        // [levelmax+1][5] reduced CFL values
   double* d_scratch = nullptr;    // standalone cmpdt partials
   size_t scratch_elems = 0;
   // lazy set_unew / fused CFL bookkeeping, per level
   std::vector<char> unew_pending;  // set_unew called, unew not yet materialised
+  std::vector<char> unew_copied;   // set_unew copied uold into unew (multi-level meshes)
   std::vector<char> unew_written;  // godunov wrote unew for the whole level
   std::vector<char> cfl_on_unew;   // d_cfl[l] holds CFL values of unew
   std::vector<char> cfl_on_uold;   // d_cfl[l] holds CFL values of uold
@@ -80,5 +95,10 @@ struct Context {
 };
 
 Context& ctx();
+
+// coarse-fine levels (rh_amr.cu)
+int build_amr_tables(int l, const TileCfg& cfg, long long gbase);
+int upload_amr_tables(int l);
+int prolong_ghosts(int l, double smallr);
 
 }  // namespace rh

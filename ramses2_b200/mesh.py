@@ -267,3 +267,90 @@ def riemann3d_state(rng, n_cells, gamma=None):
     mask = np.broadcast_to(mask, (N, N, N))
     prims = [np.where(mask, states[0][i], states[1][i]) for i in range(5)]
     return g, prim_to_cons(*prims, g)
+
+
+# ---------------------------------------------------------------------------
+# Static AMR meshes
+# ---------------------------------------------------------------------------
+def _dilate_keys(keys, r):
+    """All integer points within Chebyshev distance r of the given (n,3) keys."""
+    offs = np.array([(i, j, k) for i in range(-r, r + 1) for j in range(-r, r + 1) for k in range(-r, r + 1)],
+                    dtype=np.int64)
+    out = (keys[:, None, :] + offs[None, :, :]).reshape(-1, 3)
+    return np.unique(out, axis=0)
+
+
+def amr_mesh(levelmin, levelmax, refine, bc="outflow", boxlen=1.0, nexpand=1, box_nx=(1, 1, 1)):
+    """Properly nested static AMR mesh (nsubgrid = 1).
+
+    Level ``levelmin`` fills the box.  At each level l < levelmax, the cells
+    for which ``refine(centres (n,3), l)`` is true, dilated by ``nexpand`` cells
+    and restricted to cells at least 2 cells (in every direction) inside the
+    level's covered region, get a child oct at level l+1 - the margin that
+    interpolating a missing fine neighbour needs (father cell and its six
+    neighbours, hydro/interpol_hydro.f90:5-109).  Out-of-box neighbours do not
+    count against the margin.  Octs are stored level by level in Morton order,
+    and ``refined`` flags mark the cells that have children.
+    """
+    nb = np.array(box_nx, dtype=np.int64)
+    levels = {}
+    # level levelmin: all octs
+    no = nb << (levelmin - 1)
+    ix, iy, iz = np.meshgrid(np.arange(no[0]), np.arange(no[1]), np.arange(no[2]), indexing="ij")
+    levels[levelmin] = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], axis=1).astype(np.int64)
+    for l in range(levelmin, levelmax):
+        octs = levels[l]
+        cells = (2 * octs[:, None, :] + CELL_OFF[None, :, :]).reshape(-1, 3)
+        dx = boxlen / 2.0 ** l
+        flag = refine((cells + 0.5) * dx, l)
+        fk = cells[flag]
+        if len(fk) == 0:
+            break
+        if nexpand > 0:
+            fk = _dilate_keys(fk, nexpand)
+        ncell = nb << l
+        inbox = np.all((fk >= 0) & (fk < ncell[None, :]), axis=1)
+        fk = fk[inbox]
+        # margin: every cell within 2 of a flagged cell (inside the box) must exist at level l
+        covered = set(map(tuple, cells.tolist()))
+        ok = np.ones(len(fk), dtype=bool)
+        offs = [(i, j, k) for i in range(-2, 3) for j in range(-2, 3) for k in range(-2, 3)]
+        for n, c in enumerate(fk.tolist()):
+            for o in offs:
+                q = (c[0] + o[0], c[1] + o[1], c[2] + o[2])
+                if all(0 <= q[d] < ncell[d] for d in range(3)) and q not in covered:
+                    ok[n] = False
+                    break
+        fk = fk[ok]
+        if len(fk) == 0:
+            break
+        levels[l + 1] = np.unique(fk, axis=0)  # child oct keys at level l+1 = flagged cell coords
+    lmax = max(levels)
+    grids = []
+    for l in range(levelmin, lmax + 1):
+        k = levels[l]
+        order = np.argsort(_morton3(k[:, 0], k[:, 1], k[:, 2]), kind="stable")
+        k = k[order]
+        levels[l] = k
+        g = np.zeros(len(k), dtype=OCT_DTYPE)
+        g["ckey"] = k
+        g["lev"] = l
+        g["hkey"] = _morton3(k[:, 0], k[:, 1], k[:, 2])
+        if l < lmax:
+            child = set(map(tuple, levels[l + 1].tolist())) if (l + 1) in levels else set()
+            cells = (2 * k[:, None, :] + CELL_OFF[None, :, :])
+            ref = np.array([[tuple(c) in child for c in oc] for oc in cells.tolist()], dtype=np.uint8)
+            g["refined"] = ref
+        grids.append(g)
+    grid = np.concatenate(grids)
+    return Mesh(grid, levelmin, lmax, nsubgrid=1, boxlen=boxlen, bc=bc, box_nx=box_nx)
+
+
+def fill_amr_prim(mesh, prim_fn, gamma):
+    """Fill every level from a function of cell centres -> (rho, u, v, w, p)."""
+    for lev in range(mesh.levelmin, mesh.levelmax + 1):
+        if not mesh.noct[lev]:
+            continue
+        x = mesh.cell_centres(lev)
+        rho, u, v, w, p = prim_fn(x, lev)
+        set_level_prim(mesh, lev, rho, u, v, w, p, gamma)

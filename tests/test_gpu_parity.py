@@ -160,3 +160,79 @@ def test_one_step_fp32_bulk(case):
     err = rel_l1(out, ref)
     assert err[0] <= TOL_FP32_RHO, err
     assert np.all(err <= 1e-4), err
+
+
+# ---------------------------------------------------------------------------
+# Coarse-fine (AMR) levels
+# ---------------------------------------------------------------------------
+def amr_case(bc="outflow", itype=1, ivar=0):
+    from ramses2_b200.mesh import amr_mesh, fill_amr_prim
+
+    m = amr_mesh(4, 6, lambda x, l: np.sqrt(((x - 0.52) ** 2).sum(-1)) < 0.16, bc=bc)
+
+    def prim(x, l):
+        r = np.sqrt(((x - 0.5) ** 2).sum(-1))
+        rho = 1 + 0.5 * np.exp(-r ** 2 / 0.01)
+        p = 1 + 4 * np.exp(-r ** 2 / 0.004)
+        z = np.zeros_like(r)
+        return rho, 0.3 + z + 0.2 * np.sin(6 * x[..., 1]), -0.2 + z, 0.1 + z * 0 + 0.1 * x[..., 0], p
+
+    fill_amr_prim(m, prim, 1.4)
+    P = HydroParams.make(gamma=1.4, courant_factor=0.8, slope_type=2, riemann="hllc", interpol_type=itype,
+                         interpol_var=ivar)
+    return m, P
+
+
+def amr_step(solver, m, dt=None):
+    """One coarse step with nsubcycle=1 in amr_step.f90's order: CFL of every
+    level (the finest dt wins, amr_step.f90:588), set_unew coarse to fine, then
+    godunov + set_uold fine to coarse."""
+    lev = [l for l in range(m.levelmin, m.levelmax + 1) if m.noct[l]]
+    if dt is None:
+        dt = min(min(m.dx(l) / solver.params.smallc, solver.courant_fine(l)[4]) for l in lev)
+    for l in lev:
+        solver.set_unew(l)
+    for l in reversed(lev):
+        solver.godunov_fine(l, dt)
+        solver.set_uold(l)
+    return dt
+
+
+@pytest.mark.parametrize("bc,itype,ivar", [("outflow", 1, 0), ("periodic", 2, 1), ("reflexive", 0, 0),
+                                           ("outflow", 3, 0)])
+def test_amr_steps_fp64(bc, itype, ivar):
+    m, P = amr_case(bc, itype, ivar)
+    u0 = m.uold.copy()
+    o = oracle.OracleHydro(m, P, nthreads=NTHREADS)
+    dts = []
+    refs = []
+    for _ in range(3):
+        dts.append(amr_step(o, m))
+        refs.append(m.uold.copy())
+    m.uold[:] = u0
+    gpu = GodunovGPU(m, P, precision="fp64")
+    try:
+        for s in range(3):
+            dt = amr_step(gpu, m)
+            assert dt == pytest.approx(dts[s], rel=1e-12)
+            err = rel_l1(gpu.fetch_uold(), refs[s])
+            assert np.all(err <= TOL_FP64), (s, err)
+    finally:
+        gpu.close()
+
+
+def test_amr_step_fp32_bulk():
+    m, P = amr_case("outflow", 1, 0)
+    u0 = m.uold.copy()
+    o = oracle.OracleHydro(m, P, nthreads=NTHREADS)
+    dt = amr_step(o, m)
+    ref = m.uold.copy()
+    m.uold[:] = u0
+    gpu = GodunovGPU(m, P, precision="fp32_bulk")
+    try:
+        amr_step(gpu, m, dt)
+        err = rel_l1(gpu.fetch_uold(), ref)
+    finally:
+        gpu.close()
+    assert err[0] <= TOL_FP32_RHO, err
+    assert np.all(err <= 1e-4), err
