@@ -79,3 +79,41 @@ def dptr(a):
     """Pointer to a C-contiguous float64 numpy array."""
     assert a.dtype == np.float64 and a.flags.c_contiguous
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+RH_IC_SPLIT = 1
+RH_IC_BLAST = 2
+RH_IC_HOST = 3
+
+
+class BatchProblem(C.Structure):
+    """rh_batch_problem (include/ramses_hydro_batch.h)."""
+
+    _fields_ = [
+        ("n", C.c_int32 * 3),
+        ("ndim", C.c_int32),
+        ("bound_type", C.c_int32 * 6),
+        ("dx", C.c_double),
+        ("gamma", C.c_double),
+        ("smallr", C.c_double),
+        ("smallc", C.c_double),
+        ("courant_factor", C.c_double),
+        ("t_end", C.c_double),
+        ("max_steps", C.c_int32),
+    ]
+
+
+class BatchIC(C.Structure):
+    """rh_batch_ic (include/ramses_hydro_batch.h)."""
+
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("axis", C.c_int32),
+        ("left", C.c_double * 5),
+        ("right", C.c_double * 5),
+        ("ambient", C.c_double * 5),
+        ("p_in", C.c_double),
+        ("radius", C.c_double),
+        ("centre", C.c_double * 3),
+        ("host_uold", C.c_void_p),
+    ]

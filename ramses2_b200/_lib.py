@@ -6,7 +6,7 @@ entry point of this package raises.
 import ctypes as C
 import os
 
-from ._abi import HydroParams, MeshDesc, STATUS
+from ._abi import STATUS, BatchIC, BatchProblem, HydroParams, MeshDesc
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librh_b200.so")
@@ -41,6 +41,20 @@ SIGNATURES = {
     "rh_bench_godunov": (_i, [_i, _i, _d, _d, _d, _d, _d, _d, _i, _i, _P(C.c_float)]),
     "rh_timer_start": (_i, []),
     "rh_timer_stop": (_i, [_P(C.c_float)]),
+    # batch (include/ramses_hydro_batch.h)
+    "rh_batch_init": (_i, [_i, _i, _i, C.c_longlong]),
+    "rh_batch_free": (_i, []),
+    "rh_batch_footprint": (C.c_longlong, [_P(BatchProblem)]),
+    "rh_batch_add": (_i, [_P(BatchProblem), _P(BatchIC), _P(_i)]),
+    "rh_batch_remove": (_i, [_i]),
+    "rh_batch_step": (_i, [_i]),
+    "rh_batch_status": (_i, [_i, _P(_d), _P(_i), _P(_i), _P(_d), _P(_d)]),
+    "rh_batch_poll": (_i, [_P(_i), _P(_i), _P(_d)]),
+    "rh_batch_capacity": (_i, []),
+    "rh_batch_fetch": (_i, [_i, _P(_d)]),
+    "rh_batch_set_tile": (_i, [_i, _i, _i, _i]),
+    "rh_batch_bench": (_i, [_i, _P(C.c_float)]),
+    "rh_batch_cells": (C.c_longlong, []),
 }
 
 

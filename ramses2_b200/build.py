@@ -27,6 +27,7 @@ def _sources():
 
 def _deps():
     return _sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
+        glob.glob(os.path.join(CSRC, "*.inc")) + \
         glob.glob(os.path.join(ROOT, "include", "*.h"))
 
 

@@ -11,6 +11,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "ramses_hydro_batch.h"
 #include "rh_internal.h"
 #include "rh_launch.h"
 
@@ -415,6 +416,7 @@ int rh_finalize(void) {
   Context& c = ctx();
   if (!c.inited) return RH_OK;
   cudaStreamSynchronize(c.stream);
+  rh_batch_free();
   free_state();
   cudaFree(c.d_err);
   cudaEventDestroy(c.ev0);

@@ -1,0 +1,709 @@
+// rh_batch.cu — the batch runtime: device pool, problem admission by HBM
+// footprint, device-side initial conditions, the persistent step kernel's
+// work list, per-problem CFL/time reduction and CUDA-graph replay.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "ramses_hydro_batch.h"
+#include "rh_batch.cuh"
+#include "rh_internal.h"
+
+namespace rh {
+
+struct BatchReg {
+  BatchKey k;
+  BatchLaunchFn fn;
+  const void* func;
+  size_t smem;
+  int threads;
+};
+static std::vector<BatchReg>& batch_registry() {
+  static std::vector<BatchReg> r;
+  return r;
+}
+void register_batch_launcher(const BatchKey& k, BatchLaunchFn fn, const void* func, size_t smem, int threads) {
+  batch_registry().push_back({k, fn, func, smem, threads});
+}
+static const BatchReg* find_batch(int prec, int txo, int tyo, int minb, int slope, int riemann) {
+  for (auto& e : batch_registry())
+    if (e.k.prec == prec && e.k.txo == txo && e.k.tyo == tyo && e.k.minb == minb && e.k.slope == slope &&
+        e.k.riemann == riemann)
+      return &e;
+  return nullptr;
+}
+
+namespace {
+
+struct HostProb {
+  bool used = false;
+  rh_batch_problem p;
+  long long oct0 = 0, noct = 0;
+};
+
+struct Batch {
+  bool inited = false;
+  int precision = RH_PREC_FP64, slope = 2, riemann = 3;
+  TileCfg cfg{8, 4, 2, 16};
+  long long pool_octs = 0;
+  int parity = 0;
+  double* ud[2] = {nullptr, nullptr};
+  float* uf[2] = {nullptr, nullptr};
+  std::vector<std::pair<long long, long long>> free_list;  // [start, end) in octs
+  std::vector<HostProb> probs;
+  int cap = 0;
+  // device problem tables
+  BatchProb* d_prob = nullptr;
+  int* d_done = nullptr;
+  int* d_nstep = nullptr;
+  int* d_cur = nullptr;          // pool buffer holding each problem's current state
+  double* d_dt = nullptr;
+  double* d_t = nullptr;
+  double* d_tot = nullptr;       // [cap][5]
+  int* d_order = nullptr;
+  long long* d_woff = nullptr;
+  double* d_partial = nullptr;
+  long long partial_cap = 0;
+  unsigned long long* d_counter = nullptr;
+  int nslot = 0;
+  long long nwork = 0;
+  bool dirty = true;             // work list / graph must be rebuilt
+  cudaGraphExec_t graph = nullptr;
+  int graph_parity = 0;
+  int nblocks = 0;
+  double* d_tmp = nullptr;       // initial-CFL partials
+  long long tmp_cap = 0;
+};
+
+Batch& B() {
+  static Batch b;
+  return b;
+}
+
+int pool_bytes_per_oct(int prec) { return prec == RH_PREC_FP64 ? 2 * 320 : 2 * 192; }
+
+// ---- kernels ---------------------------------------------------------------
+
+// Initial conditions of one problem (row-major octs).
+__global__ void batch_ic_kernel(rh_batch_ic ic, BatchProb P, double* ud, float* uf, int fp32, const double* host) {
+  const long long noct = (long long)(P.ncx >> 1) * (P.ncy >> 1) * (P.ncz >> 1);
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= noct * 8) return;
+  const long long oct = i >> 3;
+  const int cell = (int)(i & 7);
+  const int nxo = P.ncx >> 1, nyo = P.ncy >> 1;
+  const int ox = (int)(oct % nxo), oy = (int)((oct / nxo) % nyo), oz = (int)(oct / ((long long)nxo * nyo));
+  const int c[3] = {2 * ox + (cell & 1), 2 * oy + ((cell >> 1) & 1), 2 * oz + ((cell >> 2) & 1)};
+  const int ncell[3] = {P.ncx, P.ncy, P.ncz};
+  double u[5];
+  if (ic.kind == RH_IC_HOST) {
+    for (int v = 0; v < 5; ++v) u[v] = host[oct * 40 + v * 8 + cell];
+  } else {
+    double q[5];
+    if (ic.kind == RH_IC_SPLIT) {
+      const bool left = c[ic.axis] < ncell[ic.axis] / 2;
+      for (int v = 0; v < 5; ++v) q[v] = left ? ic.left[v] : ic.right[v];
+    } else {
+      double r2 = 0.0;
+      for (int d = 0; d < P.ndim; ++d) {
+        const double x = (c[d] + 0.5) * P.dx - ic.centre[d];
+        r2 += x * x;
+      }
+      for (int v = 0; v < 5; ++v) q[v] = ic.ambient[v];
+      if (r2 <= ic.radius * ic.radius * (1.0 + 1e-12)) q[4] = ic.p_in;
+    }
+    u[0] = q[0];
+    u[1] = q[0] * q[1];
+    u[2] = q[0] * q[2];
+    u[3] = q[0] * q[3];
+    u[4] = q[4] / (P.gamma - 1.0) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  }
+  const long long o = P.oct0 + oct;
+  if (!fp32) {
+    for (int v = 0; v < 5; ++v) ud[o * 40 + v * 8 + cell] = u[v];
+  } else {
+    for (int v = 0; v < 4; ++v) uf[o * 32 + v * 8 + cell] = (float)u[v];
+    ud[o * 8 + cell] = u[4];
+  }
+}
+
+// courant_fine of one problem's state: per-block partials.
+__global__ void batch_cfl_kernel(BatchProb P, const double* ud, const float* uf, int fp32, double* partial) {
+  __shared__ double red[32][4];
+  const long long noct = (long long)(P.ncx >> 1) * (P.ncy >> 1) * (P.ncz >> 1);
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  LevelArgs A;
+  batch_level(P, 1.0, nullptr, A);
+  CflAcc acc;
+  if (i < noct * 8) {
+    const long long o = P.oct0 + (i >> 3);
+    const int cell = (int)(i & 7);
+    double r, m1, m2, m3, E;
+    if (!fp32) {
+      const double* p = ud + o * 40 + cell;
+      r = p[0]; m1 = p[8]; m2 = p[16]; m3 = p[24]; E = p[32];
+    } else {
+      const float* p = uf + o * 32 + cell;
+      r = p[0]; m1 = p[8]; m2 = p[16]; m3 = p[24]; E = ud[o * 8 + cell];
+    }
+    acc.add(r, m1, m2, m3, E, A);
+  }
+  double v[4] = {acc.mass, acc.ekin, acc.eint, acc.dt};
+  for (int off = 16; off > 0; off >>= 1) {
+    v[0] += __shfl_down_sync(0xffffffffu, v[0], off);
+    v[1] += __shfl_down_sync(0xffffffffu, v[1], off);
+    v[2] += __shfl_down_sync(0xffffffffu, v[2], off);
+    const double q = __shfl_down_sync(0xffffffffu, v[3], off);
+    v[3] = q < v[3] ? q : v[3];
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { red[w][0] = v[0]; red[w][1] = v[1]; red[w][2] = v[2]; red[w][3] = v[3]; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0, c = 0, d = 1e300;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      a += red[k][0]; b += red[k][1]; c += red[k][2];
+      d = red[k][3] < d ? red[k][3] : d;
+    }
+    double* out = partial + blockIdx.x * 5ll;
+    out[0] = a; out[1] = b; out[2] = c; out[3] = 0.0; out[4] = d;
+  }
+}
+
+// dt of the next step from a courant_fine result: min(dx/smallc, cell dt)
+// (newdt_fine.f90:71,103-108), cut so the problem lands on t_end.
+__device__ __forceinline__ double next_dt(const BatchProb& P, double t, double cfl_dt) {
+  double dt = P.dx / P.smallc;
+  dt = cfl_dt < dt ? cfl_dt : dt;
+  if (P.t_end > 0.0 && t + dt > P.t_end) dt = P.t_end - t;
+  return dt;
+}
+
+// Reduce the partials of n blocks into totals and (optionally) advance time.
+__device__ void reduce_block(const double* partial, long long n, double* out4) {
+  __shared__ double red[256][4];
+  double a = 0, b = 0, c = 0, d = 1e300;
+  for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+    a += partial[i * 5 + 0]; b += partial[i * 5 + 1]; c += partial[i * 5 + 2];
+    d = partial[i * 5 + 4] < d ? partial[i * 5 + 4] : d;
+  }
+  red[threadIdx.x][0] = a; red[threadIdx.x][1] = b; red[threadIdx.x][2] = c; red[threadIdx.x][3] = d;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      red[threadIdx.x][0] += red[threadIdx.x + s][0];
+      red[threadIdx.x][1] += red[threadIdx.x + s][1];
+      red[threadIdx.x][2] += red[threadIdx.x + s][2];
+      const double o = red[threadIdx.x + s][3];
+      red[threadIdx.x][3] = o < red[threadIdx.x][3] ? o : red[threadIdx.x][3];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out4[0] = red[0][0]; out4[1] = red[0][1]; out4[2] = red[0][2]; out4[3] = red[0][3];
+  }
+}
+
+// Initial CFL of one problem (no time advance).
+__global__ void batch_init_dt_kernel(BatchProb P, int id, const double* partial, long long n, double* dt,
+                                     double* tot) {
+  __shared__ double r4[4];
+  reduce_block(partial, n, r4);
+  if (threadIdx.x == 0) {
+    dt[id] = next_dt(P, 0.0, r4[3]);
+    double* o = tot + id * 5ll;
+    o[0] = r4[0]; o[1] = r4[1]; o[2] = r4[2]; o[3] = 0.0; o[4] = r4[3];
+  }
+}
+
+// After a batch step: per problem, reduce its pencils' partials (fixed
+// order), advance t and the step count, set the next dt and the done flag.
+__global__ void batch_reduce_kernel(const BatchProb* prob, const int* order, const long long* woff,
+                                    const double* partial, int* done, int* nstep, int* cur, double* dt, double* t,
+                                    double* tot, unsigned long long* counter, int parity) {
+  const int slot = blockIdx.x;
+  const int id = order[slot];
+  if (slot == 0 && threadIdx.x == 0) *counter = 0ull;
+  if (done[id]) return;
+  __shared__ double r4[4];
+  reduce_block(partial + woff[slot] * 5, woff[slot + 1] - woff[slot], r4);
+  if (threadIdx.x == 0) {
+    const BatchProb P = prob[id];
+    const double tn = t[id] + dt[id];
+    t[id] = tn;
+    const int ns = nstep[id] + 1;
+    nstep[id] = ns;
+    cur[id] = 1 - parity;
+    double* o = tot + id * 5ll;
+    o[0] = r4[0]; o[1] = r4[1]; o[2] = r4[2]; o[3] = 0.0; o[4] = r4[3];
+    const bool fin = (P.t_end > 0.0 && tn >= P.t_end * (1.0 - 1e-12)) || (P.max_steps > 0 && ns >= P.max_steps);
+    done[id] = fin ? 1 : 0;
+    dt[id] = next_dt(P, tn, r4[3]);
+  }
+}
+
+// ---- host helpers ------------------------------------------------------------
+
+int alloc_octs(long long n, long long* start) {
+  Batch& b = B();
+  for (size_t i = 0; i < b.free_list.size(); ++i) {
+    auto& f = b.free_list[i];
+    if (f.second - f.first >= n) {
+      *start = f.first;
+      f.first += n;
+      if (f.first == f.second) b.free_list.erase(b.free_list.begin() + i);
+      return RH_OK;
+    }
+  }
+  return RH_ENOMEM;
+}
+
+void free_octs(long long start, long long n) {
+  Batch& b = B();
+  b.free_list.push_back({start, start + n});
+  std::sort(b.free_list.begin(), b.free_list.end());
+  std::vector<std::pair<long long, long long>> merged;
+  for (auto& f : b.free_list) {
+    if (!merged.empty() && merged.back().second == f.first) merged.back().second = f.second;
+    else merged.push_back(f);
+  }
+  b.free_list.swap(merged);
+}
+
+BatchProb make_prob(const rh_batch_problem& p, long long oct0) {
+  Batch& b = B();
+  BatchProb P;
+  P.oct0 = oct0;
+  P.ncx = p.n[0];
+  P.ncy = p.n[1];
+  P.ncz = p.n[2];
+  for (int i = 0; i < 6; ++i) P.btype[i] = p.bound_type[i];
+  for (int d = 0; d < 3; ++d) P.periodic[d] = p.bound_type[2 * d] == RH_BOUND_PERIODIC ? 1 : 0;
+  if (p.ndim == 2) P.periodic[2] = 1;
+  P.ndim = p.ndim;
+  P.tx = (p.n[0] / 2 + b.cfg.txo - 1) / b.cfg.txo;
+  P.ty = (p.n[1] / 2 + b.cfg.tyo - 1) / b.cfg.tyo;
+  P.tz = (p.n[2] / 2 + b.cfg.lz - 1) / b.cfg.lz;
+  P.dx = p.dx;
+  P.gamma = p.gamma;
+  P.smallr = p.smallr;
+  P.smallc = p.smallc;
+  P.courant = p.courant_factor;
+  P.t_end = p.t_end;
+  P.max_steps = p.max_steps;
+  return P;
+}
+
+// Rebuild the work list (largest problems first) and the step graph.
+int rebuild() {
+  Batch& b = B();
+  Context& c = ctx();
+  RH_CUDA(cudaStreamSynchronize(c.stream));  // the tables below are read by steps in flight
+  std::vector<int> ids;
+  for (int i = 0; i < b.cap; ++i)
+    if (b.probs[i].used) ids.push_back(i);
+  std::sort(ids.begin(), ids.end(), [&](int x, int y) { return b.probs[x].noct > b.probs[y].noct; });
+  std::vector<long long> woff(ids.size() + 1, 0);
+  std::vector<BatchProb> probs(b.cap);
+  for (int i = 0; i < b.cap; ++i)
+    if (b.probs[i].used) probs[i] = make_prob(b.probs[i].p, b.probs[i].oct0);
+  for (size_t s = 0; s < ids.size(); ++s) {
+    const BatchProb& P = probs[ids[s]];
+    woff[s + 1] = woff[s] + (long long)P.tx * P.ty * P.tz;
+  }
+  b.nslot = (int)ids.size();
+  b.nwork = woff.back();
+  RH_CUDA(cudaMemcpy(b.d_prob, probs.data(), sizeof(BatchProb) * b.cap, cudaMemcpyHostToDevice));
+  cudaFree(b.d_order);
+  cudaFree(b.d_woff);
+  b.d_order = nullptr;
+  b.d_woff = nullptr;
+  RH_CUDA(cudaMalloc(&b.d_order, sizeof(int) * std::max<size_t>(1, ids.size())));
+  RH_CUDA(cudaMalloc(&b.d_woff, sizeof(long long) * woff.size()));
+  if (!ids.empty()) RH_CUDA(cudaMemcpy(b.d_order, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
+  RH_CUDA(cudaMemcpy(b.d_woff, woff.data(), sizeof(long long) * woff.size(), cudaMemcpyHostToDevice));
+  if (b.nwork > b.partial_cap) {
+    cudaFree(b.d_partial);
+    b.d_partial = nullptr;
+    RH_CUDA(cudaMalloc(&b.d_partial, sizeof(double) * 5 * b.nwork));
+    b.partial_cap = b.nwork;
+  }
+  const BatchReg* reg = find_batch(b.precision, b.cfg.txo, b.cfg.tyo, b.cfg.minb, b.slope, b.riemann);
+  if (!reg) {
+    set_error("no batch kernel for tile %dx%d minb %d slope %d riemann %d", b.cfg.txo, b.cfg.tyo, b.cfg.minb,
+              b.slope, b.riemann);
+    return RH_EINVAL;
+  }
+  RH_CUDA(cudaFuncSetAttribute(reg->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)reg->smem));
+  int per_sm = 0;
+  RH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reg->func, reg->threads, reg->smem));
+  b.nblocks = std::max(1, per_sm) * c.sm_count;
+  if (b.nwork > 0 && b.nwork < b.nblocks) b.nblocks = (int)b.nwork;
+  // graph of two steps (parity p, then 1-p), each: persistent kernel + reduction
+  if (b.graph) {
+    cudaGraphExecDestroy(b.graph);
+    b.graph = nullptr;
+  }
+  if (b.nslot > 0) {
+    cudaGraph_t g;
+    RH_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    for (int h = 0; h < 2; ++h) {
+      const int par = (b.parity + h) & 1;
+      BatchArgs A{b.d_prob, b.d_order, b.d_woff, b.nslot, b.nwork, b.cfg.txo, b.cfg.tyo, b.cfg.lz, b.d_counter,
+                  b.d_done, b.d_dt, b.d_partial, {b.ud[0], b.ud[1]}, {b.uf[0], b.uf[1]}, c.d_err};
+      cudaError_t e = reg->fn(A, par, b.nblocks, c.stream);
+      if (e != cudaSuccess) {
+        cudaStreamEndCapture(c.stream, &g);
+        return cuda_fail(e, "batch step capture");
+      }
+      batch_reduce_kernel<<<b.nslot, 256, 0, c.stream>>>(b.d_prob, b.d_order, b.d_woff, b.d_partial, b.d_done,
+                                                         b.d_nstep, b.d_cur, b.d_dt, b.d_t, b.d_tot, b.d_counter,
+                                                         par);
+    }
+    RH_CUDA(cudaStreamEndCapture(c.stream, &g));
+    RH_CUDA(cudaGraphInstantiate(&b.graph, g, 0));
+    cudaGraphDestroy(g);
+    b.graph_parity = b.parity;
+  }
+  b.dirty = false;
+  return RH_OK;
+}
+
+}  // namespace
+}  // namespace rh
+
+using namespace rh;
+
+extern "C" {
+
+int rh_batch_init(int precision, int slope, int riemann, long long pool_octs) {
+  Context& c = ctx();
+  if (!c.inited) {
+    set_error("rh_init has not been called");
+    return RH_ESTATE;
+  }
+  Batch& b = B();
+  if (b.inited) rh_batch_free();
+  if ((precision != RH_PREC_FP64 && precision != RH_PREC_FP32_BULK) || slope < 0 || slope > 2 || riemann < 1 ||
+      riemann > 3 || pool_octs < 1) {
+    set_error("rh_batch_init: bad precision/slope/riemann/pool size");
+    return RH_EINVAL;
+  }
+  b.precision = precision;
+  b.slope = slope;
+  b.riemann = riemann;
+  b.pool_octs = pool_octs;
+  b.cap = 4096;
+  for (int i = 0; i < 2; ++i) {
+    if (precision == RH_PREC_FP64) {
+      RH_CUDA(cudaMalloc(&b.ud[i], sizeof(double) * 40 * pool_octs));
+    } else {
+      RH_CUDA(cudaMalloc(&b.uf[i], sizeof(float) * 32 * pool_octs));
+      RH_CUDA(cudaMalloc(&b.ud[i], sizeof(double) * 8 * pool_octs));
+    }
+  }
+  RH_CUDA(cudaMalloc(&b.d_prob, sizeof(BatchProb) * b.cap));
+  RH_CUDA(cudaMalloc(&b.d_done, sizeof(int) * b.cap));
+  RH_CUDA(cudaMalloc(&b.d_nstep, sizeof(int) * b.cap));
+  RH_CUDA(cudaMalloc(&b.d_cur, sizeof(int) * b.cap));
+  RH_CUDA(cudaMalloc(&b.d_dt, sizeof(double) * b.cap));
+  RH_CUDA(cudaMalloc(&b.d_t, sizeof(double) * b.cap));
+  RH_CUDA(cudaMalloc(&b.d_tot, sizeof(double) * 5 * b.cap));
+  RH_CUDA(cudaMalloc(&b.d_counter, sizeof(unsigned long long)));
+  RH_CUDA(cudaMemset(b.d_counter, 0, sizeof(unsigned long long)));
+  RH_CUDA(cudaMemset(b.d_done, 0, sizeof(int) * b.cap));
+  b.probs.assign(b.cap, HostProb());
+  b.free_list = {{0, pool_octs}};
+  b.parity = 0;
+  b.dirty = true;
+  b.inited = true;
+  return RH_OK;
+}
+
+int rh_batch_free(void) {
+  Batch& b = B();
+  if (!b.inited) return RH_OK;
+  cudaStreamSynchronize(ctx().stream);
+  if (b.graph) cudaGraphExecDestroy(b.graph);
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(b.ud[i]);
+    cudaFree(b.uf[i]);
+  }
+  cudaFree(b.d_prob);
+  cudaFree(b.d_done);
+  cudaFree(b.d_nstep);
+  cudaFree(b.d_cur);
+  cudaFree(b.d_dt);
+  cudaFree(b.d_t);
+  cudaFree(b.d_tot);
+  cudaFree(b.d_order);
+  cudaFree(b.d_woff);
+  cudaFree(b.d_partial);
+  cudaFree(b.d_counter);
+  cudaFree(b.d_tmp);
+  b = Batch();
+  return RH_OK;
+}
+
+long long rh_batch_footprint(const rh_batch_problem* p) {
+  if (!p) return -1;
+  const long long noct = (long long)(p->n[0] / 2) * (p->n[1] / 2) * (p->n[2] / 2);
+  return noct * pool_bytes_per_oct(B().inited ? B().precision : RH_PREC_FP64);
+}
+
+int rh_batch_capacity(void) { return B().cap; }
+
+int rh_batch_add(const rh_batch_problem* p, const rh_batch_ic* ic, int* id) {
+  Batch& b = B();
+  Context& c = ctx();
+  if (!b.inited) {
+    set_error("rh_batch_init has not been called");
+    return RH_ESTATE;
+  }
+  if (!p || !ic || !id) {
+    set_error("rh_batch_add: null argument");
+    return RH_EINVAL;
+  }
+  for (int d = 0; d < 3; ++d)
+    if (p->n[d] < 2 || (p->n[d] & 1)) {
+      set_error("rh_batch_add: cells per edge must be even and >= 2");
+      return RH_EINVAL;
+    }
+  if ((p->ndim != 2 && p->ndim != 3) || (p->ndim == 2 && p->n[2] != 2) || !(p->dx > 0) || !(p->gamma > 1) ||
+      !(p->smallc > 0) || !(p->courant_factor > 0) || (!(p->t_end > 0) && p->max_steps <= 0)) {
+    set_error("rh_batch_add: bad ndim/dx/gamma/smallc/courant or no stopping rule (t_end or max_steps)");
+    return RH_EINVAL;
+  }
+  if (ic->kind == RH_IC_SPLIT && (ic->axis < 0 || ic->axis > 2)) {
+    set_error("rh_batch_add: split axis must be 0..2");
+    return RH_EINVAL;
+  }
+  if (ic->kind < RH_IC_SPLIT || ic->kind > RH_IC_HOST || (ic->kind == RH_IC_HOST && !ic->host_uold)) {
+    set_error("rh_batch_add: unknown initial condition");
+    return RH_EINVAL;
+  }
+  int slot = -1;
+  for (int i = 0; i < b.cap; ++i)
+    if (!b.probs[i].used) {
+      slot = i;
+      break;
+    }
+  if (slot < 0) {
+    set_error("rh_batch_add: all %d problem slots in use", b.cap);
+    return RH_EBUSY;
+  }
+  const long long noct = (long long)(p->n[0] / 2) * (p->n[1] / 2) * (p->n[2] / 2);
+  long long oct0 = 0;
+  if (alloc_octs(noct, &oct0) != RH_OK) {
+    set_error("rh_batch_add: pool full (%lld octs requested)", noct);
+    return RH_ENOMEM;
+  }
+  HostProb& hp = b.probs[slot];
+  hp.used = true;
+  hp.p = *p;
+  hp.oct0 = oct0;
+  hp.noct = noct;
+  const BatchProb P = make_prob(*p, oct0);
+  const bool fp32 = b.precision == RH_PREC_FP32_BULK;
+  double* host_dev = nullptr;
+  if (ic->kind == RH_IC_HOST) {
+    RH_CUDA(cudaMalloc(&host_dev, sizeof(double) * 40 * noct));
+    RH_CUDA(cudaMemcpyAsync(host_dev, ic->host_uold, sizeof(double) * 40 * noct, cudaMemcpyHostToDevice, c.stream));
+  }
+  const long long ncell = noct * 8;
+  batch_ic_kernel<<<(unsigned)((ncell + 255) / 256), 256, 0, c.stream>>>(*ic, P, b.ud[b.parity], b.uf[b.parity],
+                                                                          fp32 ? 1 : 0, host_dev);
+  RH_CUDA(cudaGetLastError());
+  const long long nblk = (ncell + 255) / 256;
+  if (nblk > b.tmp_cap) {
+    cudaStreamSynchronize(c.stream);
+    cudaFree(b.d_tmp);
+    b.d_tmp = nullptr;
+    RH_CUDA(cudaMalloc(&b.d_tmp, sizeof(double) * 5 * nblk));
+    b.tmp_cap = nblk;
+  }
+  batch_cfl_kernel<<<(unsigned)nblk, 256, 0, c.stream>>>(P, b.ud[b.parity], b.uf[b.parity], fp32 ? 1 : 0, b.d_tmp);
+  RH_CUDA(cudaGetLastError());
+  batch_init_dt_kernel<<<1, 256, 0, c.stream>>>(P, slot, b.d_tmp, nblk, b.d_dt, b.d_tot);
+  RH_CUDA(cudaGetLastError());
+  const int zero = 0;
+  const double dz = 0.0;
+  RH_CUDA(cudaMemcpyAsync(b.d_done + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  RH_CUDA(cudaMemcpyAsync(b.d_nstep + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  RH_CUDA(cudaMemcpyAsync(b.d_cur + slot, &b.parity, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  RH_CUDA(cudaMemcpyAsync(b.d_t + slot, &dz, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+  RH_CUDA(cudaStreamSynchronize(c.stream));
+  if (host_dev) cudaFree(host_dev);
+  b.dirty = true;
+  *id = slot;
+  return RH_OK;
+}
+
+int rh_batch_remove(int id) {
+  Batch& b = B();
+  if (!b.inited || id < 0 || id >= b.cap || !b.probs[id].used) {
+    set_error("rh_batch_remove: no problem %d", id);
+    return RH_EINVAL;
+  }
+  RH_CUDA(cudaStreamSynchronize(ctx().stream));
+  free_octs(b.probs[id].oct0, b.probs[id].noct);
+  b.probs[id] = HostProb();
+  const int one = 1;
+  RH_CUDA(cudaMemcpy(b.d_done + id, &one, sizeof(int), cudaMemcpyHostToDevice));
+  b.dirty = true;
+  return RH_OK;
+}
+
+int rh_batch_set_tile(int txo, int tyo, int minb, int lz) {
+  Batch& b = B();
+  if (!b.inited) {
+    set_error("rh_batch_init has not been called");
+    return RH_ESTATE;
+  }
+  if (!find_batch(b.precision, txo, tyo, minb, b.slope, b.riemann) || lz < 1) {
+    set_error("rh_batch_set_tile: %dx%d minb %d not compiled", txo, tyo, minb);
+    return RH_EINVAL;
+  }
+  b.cfg = TileCfg{txo, tyo, minb, lz};
+  b.dirty = true;
+  return RH_OK;
+}
+
+int rh_batch_step(int nsteps) {
+  Batch& b = B();
+  Context& c = ctx();
+  if (!b.inited) {
+    set_error("rh_batch_init has not been called");
+    return RH_ESTATE;
+  }
+  if (nsteps < 0) return RH_EINVAL;
+  if (b.dirty) {
+    int rc = rebuild();
+    if (rc) return rc;
+  }
+  if (b.nslot == 0) return RH_OK;
+  const BatchReg* reg = find_batch(b.precision, b.cfg.txo, b.cfg.tyo, b.cfg.minb, b.slope, b.riemann);
+  int done_steps = 0;
+  while (done_steps < nsteps) {
+    if (nsteps - done_steps >= 2 && b.parity == b.graph_parity) {
+      RH_CUDA(cudaGraphLaunch(b.graph, c.stream));
+      done_steps += 2;
+    } else {
+      BatchArgs A{b.d_prob, b.d_order, b.d_woff, b.nslot, b.nwork, b.cfg.txo, b.cfg.tyo, b.cfg.lz, b.d_counter,
+                  b.d_done, b.d_dt, b.d_partial, {b.ud[0], b.ud[1]}, {b.uf[0], b.uf[1]}, c.d_err};
+      RH_CUDA(reg->fn(A, b.parity, b.nblocks, c.stream));
+      batch_reduce_kernel<<<b.nslot, 256, 0, c.stream>>>(b.d_prob, b.d_order, b.d_woff, b.d_partial, b.d_done,
+                                                         b.d_nstep, b.d_cur, b.d_dt, b.d_t, b.d_tot, b.d_counter,
+                                                         b.parity);
+      RH_CUDA(cudaGetLastError());
+      b.parity ^= 1;
+      done_steps += 1;
+      continue;
+    }
+  }
+  return RH_OK;
+}
+
+int rh_batch_status(int id, double* t, int* nstep, int* done, double* dt, double* totals5) {
+  Batch& b = B();
+  Context& c = ctx();
+  if (!b.inited || id < 0 || id >= b.cap || !b.probs[id].used) {
+    set_error("rh_batch_status: no problem %d", id);
+    return RH_EINVAL;
+  }
+  RH_CUDA(cudaStreamSynchronize(c.stream));
+  if (t) RH_CUDA(cudaMemcpy(t, b.d_t + id, sizeof(double), cudaMemcpyDeviceToHost));
+  if (nstep) RH_CUDA(cudaMemcpy(nstep, b.d_nstep + id, sizeof(int), cudaMemcpyDeviceToHost));
+  if (done) RH_CUDA(cudaMemcpy(done, b.d_done + id, sizeof(int), cudaMemcpyDeviceToHost));
+  if (dt) RH_CUDA(cudaMemcpy(dt, b.d_dt + id, sizeof(double), cudaMemcpyDeviceToHost));
+  if (totals5) RH_CUDA(cudaMemcpy(totals5, b.d_tot + id * 5ll, 5 * sizeof(double), cudaMemcpyDeviceToHost));
+  return RH_OK;
+}
+
+int rh_batch_poll(int* done, int* nstep, double* t) {
+  Batch& b = B();
+  Context& c = ctx();
+  if (!b.inited) {
+    set_error("rh_batch_init has not been called");
+    return RH_ESTATE;
+  }
+  if (done) RH_CUDA(cudaMemcpyAsync(done, b.d_done, sizeof(int) * b.cap, cudaMemcpyDeviceToHost, c.stream));
+  if (nstep) RH_CUDA(cudaMemcpyAsync(nstep, b.d_nstep, sizeof(int) * b.cap, cudaMemcpyDeviceToHost, c.stream));
+  if (t) RH_CUDA(cudaMemcpyAsync(t, b.d_t, sizeof(double) * b.cap, cudaMemcpyDeviceToHost, c.stream));
+  int err = 0;
+  RH_CUDA(cudaMemcpyAsync(&err, c.d_err, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  RH_CUDA(cudaStreamSynchronize(c.stream));
+  if (err) {
+    cudaMemset(c.d_err, 0, sizeof(int));
+    set_error("device wait bound exceeded in a batch step (error word %d)", err);
+    return RH_ETIMEDOUT;
+  }
+  return RH_OK;
+}
+
+int rh_batch_fetch(int id, double* host_uold) {
+  Batch& b = B();
+  Context& c = ctx();
+  if (!b.inited || id < 0 || id >= b.cap || !b.probs[id].used || !host_uold) {
+    set_error("rh_batch_fetch: no problem %d", id);
+    return RH_EINVAL;
+  }
+  const HostProb& hp = b.probs[id];
+  RH_CUDA(cudaStreamSynchronize(c.stream));
+  int cur = 0;
+  RH_CUDA(cudaMemcpy(&cur, b.d_cur + id, sizeof(int), cudaMemcpyDeviceToHost));
+  if (b.precision == RH_PREC_FP64) {
+    RH_CUDA(cudaMemcpy(host_uold, b.ud[cur] + hp.oct0 * 40, sizeof(double) * 40 * hp.noct,
+                       cudaMemcpyDeviceToHost));
+  } else {
+    std::vector<float> f((size_t)hp.noct * 32);
+    std::vector<double> e((size_t)hp.noct * 8);
+    RH_CUDA(cudaMemcpy(f.data(), b.uf[cur] + hp.oct0 * 32, sizeof(float) * f.size(), cudaMemcpyDeviceToHost));
+    RH_CUDA(cudaMemcpy(e.data(), b.ud[cur] + hp.oct0 * 8, sizeof(double) * e.size(), cudaMemcpyDeviceToHost));
+    for (long long o = 0; o < hp.noct; ++o)
+      for (int cell = 0; cell < 8; ++cell) {
+        for (int v = 0; v < 4; ++v) host_uold[o * 40 + v * 8 + cell] = (double)f[o * 32 + v * 8 + cell];
+        host_uold[o * 40 + 32 + cell] = e[o * 8 + cell];
+      }
+  }
+  return RH_OK;
+}
+
+int rh_batch_bench(int nsteps, float* ms_per_step) {
+  Batch& b = B();
+  Context& c = ctx();
+  if (!b.inited || nsteps < 1 || !ms_per_step) {
+    set_error("rh_batch_bench: not initialised or bad arguments");
+    return RH_EINVAL;
+  }
+  if (b.dirty) {
+    int rc = rebuild();
+    if (rc) return rc;
+  }
+  RH_CUDA(cudaEventRecord(c.ev0, c.stream));
+  int rc = rh_batch_step(nsteps);
+  if (rc) return rc;
+  RH_CUDA(cudaEventRecord(c.ev1, c.stream));
+  RH_CUDA(cudaEventSynchronize(c.ev1));
+  float ms = 0;
+  RH_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+  *ms_per_step = ms / nsteps;
+  return RH_OK;
+}
+
+long long rh_batch_cells(void) {
+  Batch& b = B();
+  if (!b.inited) return 0;
+  std::vector<int> done(b.cap, 0);
+  if (cudaStreamSynchronize(ctx().stream) != cudaSuccess ||
+      cudaMemcpy(done.data(), b.d_done, sizeof(int) * b.cap, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  long long n = 0;
+  for (int i = 0; i < b.cap; ++i)
+    if (b.probs[i].used && !done[i]) n += b.probs[i].noct * 8;
+  return n;
+}
+
+}  // extern "C"

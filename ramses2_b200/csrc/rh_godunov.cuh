@@ -107,7 +107,8 @@ __device__ __forceinline__ CellMap map_coord(int g, int ncell, int periodic, int
 struct LevelArgs {
   const int4* phdr;       // per pencil: ox0, oy0, oz0, L
   const long long* poff;  // per pencil: offset of its table in ptab
-  const int* ptab;        // (L+2) x NSLOT oct indices (0-based; <0 absent)
+  const int* ptab;        // (L+2) x NSLOT oct indices (0-based; <0 absent); null: dense
+                          // row-major level (oct index = (z*nyo + y)*nxo + x, boundary-mapped)
   int npencil;
   int ncx, ncy, ncz;      // level extent in cells
   int periodic[3];
@@ -251,16 +252,49 @@ template <class G> struct Columns {
   }
 };
 
+// Dynamic shared memory of the pencil kernels and the CTA's abort flag (set
+// when an mbarrier wait gives up), referenced directly so every access is a
+// shared-memory access.
+extern __shared__ __align__(16) unsigned char rh_smem[];
+__shared__ int rh_s_abort;
+
+// Where a pencil's CFL partial goes.  The grid kernel derives it from the
+// kernel parameters at the end (nothing held in registers through the pencil);
+// the batch kernel passes the work item's slot.
+struct GridCflSink {
+  __device__ __forceinline__ bool on(const LevelArgs& A) const { return A.cfl_partial != nullptr; }
+  __device__ __forceinline__ double* out(const LevelArgs& A) const { return A.cfl_partial + (size_t)blockIdx.x * 5; }
+};
+struct SlotCflSink {
+  double* p;
+  __device__ __forceinline__ bool on(const LevelArgs&) const { return true; }
+  __device__ __forceinline__ double* out(const LevelArgs&) const { return p; }
+};
+
 // Bulk-async staging of the oct layers of a pencil.
-template <typename T, class G> struct Stager {
+template <typename T, class G, bool DENSE = false> struct Stager {
   double* stageD;
   float* stageF;
   uint64_t* bar;
   int* s_abort;
-  const int* tab;
+  const int* tab;         // pencil table (unused when DENSE)
   const double* src_d;
   const float* src_f;
   int* err;
+  int rbase;              // layers staged by earlier pencils of this CTA (barrier phases continue)
+  int4 hdr;               // pencil origin (octs) and layer count
+  int nxo, nyo, nzo;      // DENSE: level extent in octs
+  int px, py, pz;         // DENSE: periodic flags
+  __device__ __forceinline__ int rb() const { return DENSE ? rbase : 0; }
+  // Oct index at table row (layer) row, oct column slot of the pencil.
+  __device__ __forceinline__ int oct_at(int row, int slot) const {
+    if (!DENSE) return tab[(long long)row * G::NSLOT + slot];
+    auto m = [](int v, int n, int per) { return per ? ((v % n) + n) % n : (v < 0 ? 0 : (v >= n ? n - 1 : v)); };
+    const int x = m(hdr.x - 1 + slot % G::OW, nxo, px);
+    const int y = m(hdr.y - 1 + slot / G::OW, nyo, py);
+    const int z = m(hdr.z - 1 + row, nzo, pz);
+    return (z * nyo + y) * nxo + x;
+  }
   __device__ __forceinline__ void init_barriers() {
     if (threadIdx.x == 0) {
       *s_abort = 0;
@@ -271,8 +305,8 @@ template <typename T, class G> struct Stager {
   __device__ __forceinline__ void issue(int row) {
     const int t = threadIdx.x;
     if (t < G::NSLOT) {
-      const int st = row % G::NSTAGE;
-      const int oct = tab[(long long)row * G::NSLOT + t];
+      const int st = (rb() + row) % G::NSTAGE;
+      const int oct = oct_at(row, t);
       fence_proxy_async_smem();
       if (oct >= 0) {
         mbar_arrive_expect_tx(&bar[st], Store<T>::kBytes);
@@ -288,8 +322,8 @@ template <typename T, class G> struct Stager {
     }
   }
   __device__ __forceinline__ void wait(int row) {
-    const int st = row % G::NSTAGE;
-    const uint32_t par = (row / G::NSTAGE) & 1;
+    const int st = (rb() + row) % G::NSTAGE;
+    const uint32_t par = ((rb() + row) / G::NSTAGE) & 1;
     long long it = 0;
     while (!mbar_try_wait(&bar[st], par)) {
       if (*s_abort || ++it > kWaitBound) {
@@ -302,10 +336,10 @@ template <typename T, class G> struct Stager {
     }
   }
   __device__ __forceinline__ const double* slot_d(int row, int slot) const {
-    return stageD + ((size_t)(row % G::NSTAGE) * G::NSLOT + slot) * Store<T>::kSlotD;
+    return stageD + ((size_t)((rb() + row) % G::NSTAGE) * G::NSLOT + slot) * Store<T>::kSlotD;
   }
   __device__ __forceinline__ const float* slot_f(int row, int slot) const {
-    return stageF + ((size_t)(row % G::NSTAGE) * G::NSLOT + slot) * Store<T>::kSlotF;
+    return stageF + ((size_t)((rb() + row) % G::NSTAGE) * G::NSLOT + slot) * Store<T>::kSlotF;
   }
 };
 
@@ -332,248 +366,26 @@ __device__ __forceinline__ void ctoprim_f64(const double* sd, int cell, bool fx,
   q[4] = H.gm1 * eint;
 }
 
+// One pencil of the plain FP64 step for a persistent CTA: the mbarriers are
+// set up once per CTA and rbase counts the layers its earlier pencils staged.
+template <typename T, int TXO, int TYO, int SLOPE, int RIEMANN, bool AMR, bool DENSE, class Sink>
+__device__ __forceinline__ void pencil_body_f64(const LevelArgs& A, const StateArgs<T>& S, const HydroK<double>& H,
+                                                const int4 hdr, const int* tab, int rbase, const Sink sink) {
+  constexpr bool init_barriers = false;
+#include "rh_pencil_f64.inc"
+}
+
+// One pencil per CTA (the level's pencil table gives hdr and tab).
 template <typename T, int TXO, int TYO, int MINB, int SLOPE, int RIEMANN, bool AMR>
 __global__ void __launch_bounds__(Geo<T, double, TXO, TYO>::NT, MINB)
 godunov_pencil_kernel(const LevelArgs A, const StateArgs<T> S, const HydroK<double> H) {
-  using G = Geo<T, double, TXO, TYO>;
-  extern __shared__ __align__(16) unsigned char smem[];
-  double* Qb = reinterpret_cast<double*>(smem + G::oQ);    // [2][5][NLC]
-  double* FS = reinterpret_cast<double*>(smem + G::oFS);   // [10][NRC]: qp_x(5), qp_y(5)
-  double* FXY = reinterpret_cast<double*>(smem + G::oFX);  // [2][5][NRC]: x then y fluxes
-  double* red = reinterpret_cast<double*>(smem + G::oRed);
-  int* entb = reinterpret_cast<int*>(smem + G::oAmr);                    // AMR: entry of plane k
-  uint32_t* stb = reinterpret_cast<uint32_t*>(smem + G::oAmr + G::NRC * sizeof(int));  // AMR: status bits
-  __shared__ int s_abort;
-
-  const int t = threadIdx.x;
-  const int pencil = blockIdx.x;
-  const int4 hdr = A.phdr[pencil];
-  const int ox0 = hdr.x, oy0 = hdr.y, oz0 = hdr.z, L = hdr.w;
-  const int CZ = 2 * L;
-  const int* tab = A.ptab + A.poff[pencil];
-  Columns<G> col;
-  col.init(t, ox0, oy0, A);
-  Stager<T, G> stg{reinterpret_cast<double*>(smem + G::oStageD), reinterpret_cast<float*>(smem + G::oStageF),
-                   reinterpret_cast<uint64_t*>(smem + G::oBar), &s_abort, tab, S.uold_d, S.uold_f, A.err};
-  stg.init_barriers();
-  __syncthreads();
-  stg.issue(0);
-  stg.issue(1);
-  const bool active = t < G::NRC;
-  auto zmap = [&](int p) { return map_coord(2 * oz0 + p, A.ncz, A.periodic[2], A.btype[4], A.btype[5]); };
-
-  // Convert plane p: own column into (q, 1/rho, U) and the plane buffer; the
-  // outer column (if this thread owns one) into the plane buffer only.
-  auto convert = [&](int p, double* q, double& ir, double* U, bool to_buffer) {
-    const int row = (p >> 1) + 1;
-    const CellMap mz = zmap(p);
-    double* Qp = Qb + (size_t)(p & 1) * 5 * G::NLC;
-    if (active) {
-      ctoprim_f64(stg.slot_d(row, col.slot), col.mx.parity + 2 * col.my.parity + 4 * mz.parity, col.mx.flip,
-                  col.my.flip, mz.flip, H, q, ir, U);
-      if (to_buffer) {
-#pragma unroll
-        for (int n = 0; n < 5; ++n) Qp[n * G::NLC + col.lc] = q[n];
-      }
-    }
-    if (to_buffer && col.has_outer) {
-      double qo[5], iro, Uo[5];
-      ctoprim_f64(stg.slot_d(row, col.oslot), col.omx.parity + 2 * col.omy.parity + 4 * mz.parity, col.omx.flip,
-                  col.omy.flip, mz.flip, H, qo, iro, Uo);
-#pragma unroll
-      for (int n = 0; n < 5; ++n) Qp[n * G::NLC + col.olc] = qo[n];
-    }
-  };
-  // AMR: table entry and status bits of the own cell at plane p
-  auto status = [&](int p, int& ent) -> uint32_t {
-    const int row = (p >> 1) + 1;
-    const CellMap mz = zmap(p);
-    ent = tab[(long long)row * G::NSLOT + col.slot];
-    const int gz = 2 * oz0 + p;
-    const bool in_dom = col.in_dom_xy && gz >= 0 && gz < A.ncz;
-    const bool upd = col.interior && in_dom && p >= 0 && p < CZ;
-    return amr_bits(A, ent, col.mx.parity + 2 * col.my.parity + 4 * mz.parity, upd, in_dom);
-  };
-
-  double qa[5], qb[5], qc[5], irb = 0, irc = 0;  // own column, planes k-1, k, k+1
-  double Uk[5], Uk1[5];                          // uold of planes k, k+1
-  double qmx[5], qmy[5], qmz_prev[5], fz_prev[5], up[5];
-  int ea = -1, eb = -1, ec = -1;                 // AMR: entries of planes k-1, k, k+1
-  uint32_t sa = 0, sb = 0, sc = 0;               // AMR: status bits of planes k-1, k, k+1
-  CflAcc acc;
-#pragma unroll
-  for (int n = 0; n < 5; ++n) { qmz_prev[n] = 0; fz_prev[n] = 0; up[n] = 0; Uk[n] = 0; Uk1[n] = 0; qc[n] = 0; }
-
-  // prologue: planes -2 and -1 (table row 0)
-  stg.wait(0);
-  {
-    double ira;
-    convert(-2, qa, ira, Uk1, false);
-  }
-  convert(-1, qb, irb, Uk1, true);
-  if (AMR && active) sb = status(-1, eb);
-  __syncthreads();
-  if (L + 1 >= 2) stg.issue(2);
-
-  for (int k = -1; k <= CZ; ++k) {
-    // (A) primitive variables of plane k+1
-    {
-      const int p = k + 1;
-      if ((p & 1) == 0) stg.wait((p >> 1) + 1);
-      convert(p, qc, irc, Uk1, true);
-      if (AMR && active) sc = status(p, ec);
-    }
-    // (C) slopes, predictor and interface states of plane k
-    double fz[5] = {0, 0, 0, 0, 0};
-    if (active) {
-      const double* Qk = Qb + (size_t)(k & 1) * 5 * G::NLC;
-      double xm[5], xp[5], ym[5], yp[5];
-#pragma unroll
-      for (int n = 0; n < 5; ++n) {
-        xm[n] = Qk[n * G::NLC + col.lc - 1];
-        xp[n] = Qk[n * G::NLC + col.lc + 1];
-        ym[n] = Qk[n * G::NLC + col.lc - G::LW];
-        yp[n] = Qk[n * G::NLC + col.lc + G::LW];
-      }
-      double d[3][5];
-#pragma unroll
-      for (int n = 0; n < 5; ++n) {
-        d[0][n] = limited_slope<double, SLOPE>(xm[n], qb[n], xp[n], H);
-        d[1][n] = limited_slope<double, SLOPE>(ym[n], qb[n], yp[n], H);
-        d[2][n] = limited_slope<double, SLOPE>(qa[n], qb[n], qc[n], H);
-      }
-      if (SLOPE > 0) {
-        d[0][1] = momentum_bound(d[0][1], xm[0], xm[1], qb[1], xp[0], xp[1], irb, H);
-        d[1][2] = momentum_bound(d[1][2], ym[0], ym[2], qb[2], yp[0], yp[2], irb, H);
-        d[2][3] = momentum_bound(d[2][3], qa[0], qa[3], qb[3], qc[0], qc[3], irb, H);
-      }
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int n = 0; n < 5; ++n) d[a][n] = 0.5 * d[a][n];
-      double qm[3][5], qp[3][5];
-      trace_cell(qb, irb, d, qm, qp, H);
-#pragma unroll
-      for (int n = 0; n < 5; ++n) {
-        FS[n * G::NRC + t] = qp[0][n];
-        FS[(5 + n) * G::NRC + t] = qp[1][n];
-        qmx[n] = qm[0][n];
-        qmy[n] = qm[1][n];
-      }
-      if (AMR) {
-        entb[t] = eb;
-        stb[t] = sb;
-      }
-      // z interface k-1/2: left = qm_z(k-1), right = qp_z(k); rotation (r,w,u,v,p)
-      if (col.interior && k >= 0) {
-        const double ql[5] = {qmz_prev[0], qmz_prev[3], qmz_prev[1], qmz_prev[2], qmz_prev[4]};
-        const double qr[5] = {qp[2][0], qp[2][3], qp[2][1], qp[2][2], qp[2][4]};
-        double f[5];
-        riemann_dtdx<double, RIEMANN>(ql, qr, f, H);
-        fz[0] = f[0]; fz[3] = f[1]; fz[1] = f[2]; fz[2] = f[3]; fz[4] = f[4];
-        if (AMR) {
-          if ((sa | sb) & 1u) {
-#pragma unroll
-            for (int n = 0; n < 5; ++n) fz[n] = 0.0;
-          }
-          if ((sa & 2u) && (sb & 4u)) coarse_add_f64(A, S.unew_d, eb, fz, 1.0);
-          if ((sa & 4u) && (sb & 2u)) coarse_add_f64(A, S.unew_d, ea, fz, -1.0);
-        }
-      }
-#pragma unroll
-      for (int n = 0; n < 5; ++n) qmz_prev[n] = qm[2][n];
-    }
-    __syncthreads();  // S2: interface states of plane k published
-    if (k >= 0 && (k & 1) == 0 && k / 2 + 3 <= L + 1) stg.issue(k / 2 + 3);
-    // (D) x flux at the right face and y flux at the top face of the own cell
-    const bool plane_ok = k >= 0 && k < CZ;
-    if (active && plane_ok) {
-      if (col.rx >= -1 && col.rx < G::CX && col.ry >= 0 && col.ry < G::CY) {
-        const double qr[5] = {FS[0 * G::NRC + t + 1], FS[1 * G::NRC + t + 1], FS[2 * G::NRC + t + 1],
-                              FS[3 * G::NRC + t + 1], FS[4 * G::NRC + t + 1]};
-        double f[5];
-        riemann_dtdx<double, RIEMANN>(qmx, qr, f, H);
-        if (AMR) {
-          const uint32_t bl = stb[t], br = stb[t + 1];
-          if ((bl | br) & 1u) {
-#pragma unroll
-            for (int n = 0; n < 5; ++n) f[n] = 0.0;
-          }
-          if ((bl & 2u) && (br & 4u)) coarse_add_f64(A, S.unew_d, entb[t + 1], f, 1.0);
-          if ((bl & 4u) && (br & 2u)) coarse_add_f64(A, S.unew_d, entb[t], f, -1.0);
-        }
-#pragma unroll
-        for (int n = 0; n < 5; ++n) FXY[n * G::NRC + t] = f[n];
-      }
-      if (col.ry >= -1 && col.ry < G::CY && col.rx >= 0 && col.rx < G::CX) {
-        const int tn = t + G::RW;
-        const double ql[5] = {qmy[0], qmy[2], qmy[1], qmy[3], qmy[4]};
-        const double qr[5] = {FS[5 * G::NRC + tn], FS[7 * G::NRC + tn], FS[6 * G::NRC + tn], FS[8 * G::NRC + tn],
-                              FS[9 * G::NRC + tn]};
-        double f[5];
-        riemann_dtdx<double, RIEMANN>(ql, qr, f, H);
-        double fy[5] = {f[0], f[2], f[1], f[3], f[4]};
-        if (AMR) {
-          const uint32_t bl = stb[t], br = stb[tn];
-          if ((bl | br) & 1u) {
-#pragma unroll
-            for (int n = 0; n < 5; ++n) fy[n] = 0.0;
-          }
-          if ((bl & 2u) && (br & 4u)) coarse_add_f64(A, S.unew_d, entb[tn], fy, 1.0);
-          if ((bl & 4u) && (br & 2u)) coarse_add_f64(A, S.unew_d, entb[t], fy, -1.0);
-        }
-        double* FY = FXY + 5 * G::NRC;
-#pragma unroll
-        for (int n = 0; n < 5; ++n) FY[n * G::NRC + t] = fy[n];
-      }
-    }
-    __syncthreads();  // S3: fluxes of plane k published
-    // (E) finish plane k-1 with its z differences, start plane k
-    if (active && col.interior) {
-      const int pk = k - 1;
-      if (pk >= 0 && pk < CZ) {
-        const int gz = 2 * oz0 + pk;
-        const int oct = tab[(long long)((pk >> 1) + 1) * G::NSLOT + col.slot];
-        if (col.in_domain_xy && gz < A.ncz && oct >= 0 && oct < A.ghost_base) {
-          const int cell = (col.rx & 1) + 2 * (col.ry & 1) + 4 * (pk & 1);
-          double un[5];
-#pragma unroll
-          for (int n = 0; n < 5; ++n) un[n] = up[n] + (fz_prev[n] - fz[n]);
-          double* o = S.unew_d + (size_t)oct * 40 + cell;
-          o[0] = un[0]; o[8] = un[1]; o[16] = un[2]; o[24] = un[3]; o[32] = un[4];
-          if (A.cfl_partial && !(AMR && (sa & 1u))) acc.add(un[0], un[1], un[2], un[3], un[4], A);
-        }
-      }
-      if (plane_ok) {
-        const double* FX = FXY;
-        const double* FY = FXY + 5 * G::NRC;
-        double base[5];
-#pragma unroll
-        for (int n = 0; n < 5; ++n) base[n] = Uk[n];
-        if (AMR && A.accumulate) {
-          // unew holds uold plus the finer level's coarse corrections
-          const int oct = tab[(long long)((k >> 1) + 1) * G::NSLOT + col.slot];
-          if (col.in_domain_xy && 2 * oz0 + k < A.ncz && oct >= 0 && oct < A.ghost_base) {
-            const int cell = (col.rx & 1) + 2 * (col.ry & 1) + 4 * (k & 1);
-            const double* o = S.unew_d + (size_t)oct * 40 + cell;
-#pragma unroll
-            for (int n = 0; n < 5; ++n) base[n] = o[8 * n];
-          }
-        }
-#pragma unroll
-        for (int n = 0; n < 5; ++n) {
-          const double u0 = base[n] + (FX[n * G::NRC + t - 1] - FX[n * G::NRC + t]);
-          up[n] = u0 + (FY[n * G::NRC + t - G::RW] - FY[n * G::NRC + t]);
-        }
-      }
-    }
-#pragma unroll
-    for (int n = 0; n < 5; ++n) { fz_prev[n] = fz[n]; Uk[n] = Uk1[n]; qa[n] = qb[n]; qb[n] = qc[n]; }
-    irb = irc;
-    ea = eb; eb = ec;
-    sa = sb; sb = sc;
-  }
-  if (A.cfl_partial) cfl_block_reduce<G::NWARP>(acc, red, A.cfl_partial + (size_t)pencil * 5);
+  constexpr bool DENSE = false;
+  constexpr bool init_barriers = true;
+  constexpr int rbase = 0;
+  const GridCflSink sink{};
+  const int4 hdr = A.phdr[blockIdx.x];
+  const int* tab = A.ptab + A.poff[blockIdx.x];
+#include "rh_pencil_f64.inc"
 }
 
 }  // namespace rh

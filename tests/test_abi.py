@@ -34,7 +34,7 @@ def test_library_builds_and_loads():
 def test_every_declared_symbol_is_exported():
     L = lib()
     names = declared_symbols()
-    assert len(names) >= 19, names
+    assert len(names) >= 32, names
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
 
@@ -60,3 +60,15 @@ def test_ext_tile_registry_lists_compiled_shapes():
     n32 = L.rh_list_tiles(1, tx, ty, mb, 16)
     assert n32 >= 3
     assert {mb[i] for i in range(min(n32, 16))} >= {1, 2}
+
+
+def test_batch_calls_before_init_report_state_errors():
+    from ramses2_b200._abi import BatchIC, BatchProblem
+
+    L = lib()
+    assert L.rh_batch_init(0, 2, 3, 1024) == 4  # RH_ESTATE: rh_init not called
+    pid = C.c_int()
+    p, ic = BatchProblem(), BatchIC()
+    assert L.rh_batch_add(C.byref(p), C.byref(ic), C.byref(pid)) == 4
+    assert L.rh_batch_step(1) == 4
+    assert L.rh_batch_free() == 0
