@@ -69,8 +69,12 @@ int rh_batch_poll(int* done, int* nstep, double* t);
 int rh_batch_capacity(void);
 /* Copy a problem's current state to the host, reference layout, row-major octs. */
 int rh_batch_fetch(int id, double* host_uold);
-/* Tile of the batch kernel (compiled shapes: rh_list_tiles). */
+/* Tile of the batch kernel (one of the compiled shapes rh_batch_list_tiles
+ * returns; lz = oct layers per pencil). */
 int rh_batch_set_tile(int txo, int tyo, int minb, int lz);
+/* Compiled batch-kernel shapes of a precision: writes up to max entries,
+ * returns how many exist. */
+int rh_batch_list_tiles(int precision, int* txo, int* tyo, int* minb, int max);
 /* Device time of nsteps batch steps (CUDA events), milliseconds per step. */
 int rh_batch_bench(int nsteps, float* ms_per_step);
 /* Cells updated by one batch step over the unfinished problems. */

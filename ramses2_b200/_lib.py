@@ -53,6 +53,7 @@ SIGNATURES = {
     "rh_batch_capacity": (_i, []),
     "rh_batch_fetch": (_i, [_i, _P(_d)]),
     "rh_batch_set_tile": (_i, [_i, _i, _i, _i]),
+    "rh_batch_list_tiles": (_i, [_i, _P(_i), _P(_i), _P(_i), _i]),
     "rh_batch_bench": (_i, [_i, _P(C.c_float)]),
     "rh_batch_cells": (C.c_longlong, []),
 }

@@ -153,6 +153,31 @@ class Batch:
     def set_tile(self, txo, tyo, minb, lz):
         check(self.L.rh_batch_set_tile(int(txo), int(tyo), int(minb), int(lz)), "rh_batch_set_tile")
 
+    def tiles(self):
+        """Compiled (txo, tyo, minb) shapes of the batch kernel at this precision."""
+        tx, ty, mb = (C.c_int * 64)(), (C.c_int * 64)(), (C.c_int * 64)()
+        n = self.L.rh_batch_list_tiles(self.precision, tx, ty, mb, 64)
+        return [(tx[i], ty[i], mb[i]) for i in range(min(n, 64))]
+
+    def tune(self, lz_choices=(8, 16, 32), nsteps=2, reps=3, log=None):
+        """Autotune the batch kernel on the problems currently in the batch:
+        time every compiled (txo, tyo, minb) x lz with CUDA events (median of
+        ``reps`` runs of ``nsteps`` steps; the problems advance meanwhile, so
+        give them a stopping rule far away), keep the fastest selected and
+        return (best, table)."""
+        table = []
+        for (tx, ty, mb) in self.tiles():
+            for lz in lz_choices:
+                self.set_tile(tx, ty, mb, lz)
+                self.bench(1)  # rebuilds the work list and the step graph
+                ms = float(np.median([self.bench(nsteps) for _ in range(reps)]))
+                table.append({"txo": tx, "tyo": ty, "minb": mb, "lz": lz, "ms": ms})
+                if log:
+                    log("batch autotune %dx%d minb=%d lz=%d: %.3f ms/step" % (tx, ty, mb, lz, ms))
+        best = min(table, key=lambda r: r["ms"])
+        self.set_tile(best["txo"], best["tyo"], best["minb"], best["lz"])
+        return best, table
+
     def bench(self, nsteps):
         ms = C.c_float()
         check(self.L.rh_batch_bench(int(nsteps), C.byref(ms)), "rh_batch_bench")
@@ -164,3 +189,41 @@ class Batch:
 
     def close(self):
         check(self.L.rh_batch_free(), "rh_batch_free")
+
+
+def random_state(rng, gamma):
+    """Primitive (rho, u, v, w, p): rho log-uniform in [1e-3, 1e3], p
+    log-uniform in [1e-4, 1e2], |v| uniform in [0, 3] sound speeds, random direction."""
+    rho = 10 ** rng.uniform(-3, 3)
+    p = 10 ** rng.uniform(-4, 2)
+    cs = np.sqrt(gamma * p / rho)
+    d = rng.standard_normal(3)
+    d *= rng.uniform(0, 3) * cs / np.linalg.norm(d)
+    return [rho, d[0], d[1], d[2], p]
+
+
+def riemann_blast_ensemble(n_problems=1024, seed=20261203, sides=(16, 32, 48, 64, 96, 128), steps=50,
+                           blast_fraction=0.25):
+    """Independent 3D Riemann and blast problems of uneven size: cubic boxes
+    with sides drawn uniformly from ``sides`` (unit box, outflow), gamma
+    uniform in [1.1, 1.67]; a Riemann problem splits two random states along a
+    random axis, a blast puts a pressure 100x above the larger of the two
+    inside a sphere of radius 0.05-0.15 around a random centre.  Returns a list
+    of (rh_batch_problem, rh_batch_ic)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_problems):
+        s = int(rng.choice(sides))
+        g = float(rng.uniform(1.1, 1.67))
+        a, b = random_state(rng, g), random_state(rng, g)
+        p = problem((s, s, s), dx=1.0 / s, bc="outflow", gamma=g, courant_factor=0.8, max_steps=steps)
+        if rng.uniform() < blast_fraction:
+            ic = ic_blast(a, 100.0 * max(a[4], b[4]), rng.uniform(0.05, 0.15), rng.uniform(0.3, 0.7, 3))
+        else:
+            ic = ic_split(int(rng.integers(0, 3)), a, b)
+        out.append((p, ic))
+    return out
+
+
+def ensemble_octs(ensemble):
+    return sum((p.n[0] // 2) * (p.n[1] // 2) * (p.n[2] // 2) for p, _ in ensemble)

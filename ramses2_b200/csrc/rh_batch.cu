@@ -562,7 +562,7 @@ int rh_batch_set_tile(int txo, int tyo, int minb, int lz) {
     set_error("rh_batch_init has not been called");
     return RH_ESTATE;
   }
-  if (!find_batch(b.precision, txo, tyo, minb, b.slope, b.riemann) || lz < 1) {
+  if (!find_batch(b.precision, txo, tyo, minb, b.slope, b.riemann) || lz < 1 || lz > kBatchMaxLz) {
     set_error("rh_batch_set_tile: %dx%d minb %d not compiled", txo, tyo, minb);
     return RH_EINVAL;
   }
@@ -691,6 +691,20 @@ int rh_batch_bench(int nsteps, float* ms_per_step) {
   RH_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
   *ms_per_step = ms / nsteps;
   return RH_OK;
+}
+
+int rh_batch_list_tiles(int precision, int* txo, int* tyo, int* minb, int max) {
+  int n = 0;
+  for (auto& e : batch_registry()) {
+    if (e.k.prec != precision || e.k.slope != 2 || e.k.riemann != 3) continue;
+    if (n < max) {
+      if (txo) txo[n] = e.k.txo;
+      if (tyo) tyo[n] = e.k.tyo;
+      if (minb) minb[n] = e.k.minb;
+    }
+    ++n;
+  }
+  return n;
 }
 
 long long rh_batch_cells(void) {

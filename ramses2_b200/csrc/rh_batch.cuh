@@ -6,6 +6,9 @@
 
 namespace rh {
 
+constexpr int kBatchMaxLz = 64;      // most oct layers of one batch pencil
+constexpr int kBatchMaxSlots = 100;  // most oct columns (tile + halo) of one batch pencil
+
 // Static description of one problem in the device pool.
 struct BatchProb {
   long long oct0;           // first oct of the problem in the pool
@@ -97,10 +100,37 @@ template <class V> __device__ __forceinline__ void batch_hydro(const BatchProb& 
   H.grav[0] = H.grav[1] = H.grav[2] = b(0.0);
 }
 
+// Constants of the CTA's current work item, in shared memory: the pencil
+// body reads them where it uses them instead of holding them in registers.
+__shared__ LevelArgs rh_bA;
+__shared__ StateArgs<double> rh_bS64;
+__shared__ StateArgs<float> rh_bS32;
+__shared__ HydroK<double> rh_bH64;
+__shared__ HydroK<float2> rh_bH32;
+__shared__ double* rh_b_out;
+__shared__ int4 rh_b_hdr;
+__shared__ int rh_b_tab[kBatchMaxSlots + kBatchMaxLz + 2];  // dense oct offsets: xy per slot, z per row
+
+// One pencil of the current work item.  Kept out of line so the persistent
+// loop around it does not stretch the body's register live ranges.
+template <typename T, int TXO, int TYO, int SLOPE, int RIEMANN>
+__device__ __noinline__ void batch_pencil(int rbase) {
+  const int4 hdr = rh_b_hdr;
+  if constexpr (sizeof(T) == 8) {
+    pencil_body_f64<T, TXO, TYO, SLOPE, RIEMANN, false, true>(rh_bA, rh_bS64, rh_bH64, hdr, rh_b_tab, rbase,
+                                                              SlotCflSink{&rh_b_out});
+  } else {
+    pencil_body_f32<TXO, TYO, SLOPE, RIEMANN, false, true>(rh_bA, rh_bS32, rh_bH32, hdr, rh_b_tab, rbase,
+                                                           SlotCflSink{&rh_b_out});
+  }
+}
+
 template <typename T, typename V, int TXO, int TYO, int MINB, int SLOPE, int RIEMANN>
 __global__ void __launch_bounds__(Geo<T, V, TXO, TYO>::NT, MINB) batch_step_kernel(const BatchArgs B, int parity) {
   using G = Geo<T, V, TXO, TYO>;
+  static_assert(G::NSLOT <= kBatchMaxSlots, "tile too wide for the dense offset table");
   __shared__ long long s_w;
+  __shared__ int s_skip;
   if (threadIdx.x == 0) {
     rh_s_abort = 0;
     uint64_t* bar = reinterpret_cast<uint64_t*>(rh_smem + G::oBar);
@@ -109,44 +139,61 @@ __global__ void __launch_bounds__(Geo<T, V, TXO, TYO>::NT, MINB) batch_step_kern
   }
   int rbase = 0;
   for (;;) {
-    __syncthreads();
-    if (threadIdx.x == 0) s_w = (long long)atomicAdd(B.counter, 1ull);
-    __syncthreads();
-    const long long w = s_w;
-    if (w >= B.nwork) break;
-    const int slot = batch_slot(B.woff, B.nslot, w);
-    const int pid = B.order[slot];
-    if (B.done[pid]) continue;
-    const BatchProb P = B.prob[pid];
-    const double dt = B.dt[pid];
-    const long long li = w - B.woff[slot];
-    const int bx = (int)(li % P.tx), by = (int)((li / P.tx) % P.ty), bz = (int)(li / ((long long)P.tx * P.ty));
-    const int nzo = P.ncz >> 1;
-    const int4 hdr = make_int4(bx * B.txo, by * B.tyo, bz * B.lz, min(B.lz, nzo - bz * B.lz));
-    LevelArgs A;
-    batch_level(P, dt, B.err, A);
-    StateArgs<T> S;
-    if (sizeof(T) == 8) {
-      S.uold_d = B.ud[parity] + P.oct0 * 40;
-      S.unew_d = B.ud[1 - parity] + P.oct0 * 40;
-      S.uold_f = nullptr;
-      S.unew_f = nullptr;
-    } else {
-      S.uold_d = B.ud[parity] + P.oct0 * 8;
-      S.unew_d = B.ud[1 - parity] + P.oct0 * 8;
-      S.uold_f = B.uf[parity] + P.oct0 * 32;
-      S.unew_f = B.uf[1 - parity] + P.oct0 * 32;
+    __syncthreads();  // the previous pencil is finished with the work-item constants
+    if (threadIdx.x == 0) {
+      const long long w = (long long)atomicAdd(B.counter, 1ull);
+      s_w = w;
+      s_skip = 1;
+      if (w < B.nwork) {
+        const int slot = batch_slot(B.woff, B.nslot, w);
+        const int pid = B.order[slot];
+        if (!B.done[pid]) {
+          s_skip = 0;
+          rh_b_out = B.partial + w * 5;
+          const BatchProb P = B.prob[pid];
+          const double dt = B.dt[pid];
+          const long long li = w - B.woff[slot];
+          const int bx = (int)(li % P.tx), by = (int)((li / P.tx) % P.ty);
+          const int bz = (int)(li / ((long long)P.tx * P.ty));
+          const int nzo = P.ncz >> 1;
+          rh_b_hdr = make_int4(bx * B.txo, by * B.tyo, bz * B.lz, min(B.lz, nzo - bz * B.lz));
+          batch_level(P, dt, B.err, rh_bA);
+          if constexpr (sizeof(T) == 8) {
+            rh_bS64.uold_d = B.ud[parity] + P.oct0 * 40;
+            rh_bS64.unew_d = B.ud[1 - parity] + P.oct0 * 40;
+            rh_bS64.uold_f = nullptr;
+            rh_bS64.unew_f = nullptr;
+            batch_hydro<double>(P, dt, rh_bH64);
+          } else {
+            rh_bS32.uold_d = B.ud[parity] + P.oct0 * 8;
+            rh_bS32.unew_d = B.ud[1 - parity] + P.oct0 * 8;
+            rh_bS32.uold_f = B.uf[parity] + P.oct0 * 32;
+            rh_bS32.unew_f = B.uf[1 - parity] + P.oct0 * 32;
+            batch_hydro<float2>(P, dt, rh_bH32);
+          }
+        }
+      }
     }
-    HydroK<V> H;
-    batch_hydro<V>(P, dt, H);
-    if constexpr (sizeof(T) == 8) {
-      pencil_body_f64<T, TXO, TYO, SLOPE, RIEMANN, false, true>(A, S, H, hdr, nullptr, rbase,
-                                                                SlotCflSink{B.partial + w * 5});
-    } else {
-      pencil_body_f32<TXO, TYO, SLOPE, RIEMANN, false, true>(A, S, H, hdr, nullptr, rbase,
-                                                             SlotCflSink{B.partial + w * 5});
+    __syncthreads();
+    if (s_w >= B.nwork) break;
+    if (s_skip) continue;
+    {
+      // oct index of (row, slot) = tab[NSLOT + row] + tab[slot], boundary-mapped
+      const int4 hdr = rh_b_hdr;
+      const int nx = rh_bA.ncx >> 1, ny = rh_bA.ncy >> 1, nz = rh_bA.ncz >> 1;
+      auto m = [](int v, int n, int per) { return per ? ((v % n) + n) % n : (v < 0 ? 0 : (v >= n ? n - 1 : v)); };
+      for (int i = threadIdx.x; i < G::NSLOT + hdr.w + 2; i += G::NT) {
+        if (i < G::NSLOT) {
+          rh_b_tab[i] = m(hdr.y - 1 + i / G::OW, ny, rh_bA.periodic[1]) * nx +
+                        m(hdr.x - 1 + i % G::OW, nx, rh_bA.periodic[0]);
+        } else {
+          rh_b_tab[i] = m(hdr.z - 1 + (i - G::NSLOT), nz, rh_bA.periodic[2]) * (nx * ny);
+        }
+      }
+      __syncthreads();
     }
-    rbase += hdr.w + 2;
+    batch_pencil<T, TXO, TYO, SLOPE, RIEMANN>(rbase);
+    rbase += rh_b_hdr.w + 2;
   }
 }
 

@@ -107,8 +107,7 @@ __device__ __forceinline__ CellMap map_coord(int g, int ncell, int periodic, int
 struct LevelArgs {
   const int4* phdr;       // per pencil: ox0, oy0, oz0, L
   const long long* poff;  // per pencil: offset of its table in ptab
-  const int* ptab;        // (L+2) x NSLOT oct indices (0-based; <0 absent); null: dense
-                          // row-major level (oct index = (z*nyo + y)*nxo + x, boundary-mapped)
+  const int* ptab;        // (L+2) x NSLOT oct indices (0-based; <0 absent)
   int npencil;
   int ncx, ncy, ncz;      // level extent in cells
   int periodic[3];
@@ -266,9 +265,9 @@ struct GridCflSink {
   __device__ __forceinline__ double* out(const LevelArgs& A) const { return A.cfl_partial + (size_t)blockIdx.x * 5; }
 };
 struct SlotCflSink {
-  double* p;
+  double* const* p;  // shared-memory slot holding the output address
   __device__ __forceinline__ bool on(const LevelArgs&) const { return true; }
-  __device__ __forceinline__ double* out(const LevelArgs&) const { return p; }
+  __device__ __forceinline__ double* out(const LevelArgs&) const { return *p; }
 };
 
 // Bulk-async staging of the oct layers of a pencil.
@@ -277,23 +276,16 @@ template <typename T, class G, bool DENSE = false> struct Stager {
   float* stageF;
   uint64_t* bar;
   int* s_abort;
-  const int* tab;         // pencil table (unused when DENSE)
+  const int* tab;         // pencil table; DENSE: [NSLOT] xy offsets then [L+2] z offsets
   const double* src_d;
   const float* src_f;
   int* err;
   int rbase;              // layers staged by earlier pencils of this CTA (barrier phases continue)
-  int4 hdr;               // pencil origin (octs) and layer count
-  int nxo, nyo, nzo;      // DENSE: level extent in octs
-  int px, py, pz;         // DENSE: periodic flags
   __device__ __forceinline__ int rb() const { return DENSE ? rbase : 0; }
   // Oct index at table row (layer) row, oct column slot of the pencil.
   __device__ __forceinline__ int oct_at(int row, int slot) const {
     if (!DENSE) return tab[(long long)row * G::NSLOT + slot];
-    auto m = [](int v, int n, int per) { return per ? ((v % n) + n) % n : (v < 0 ? 0 : (v >= n ? n - 1 : v)); };
-    const int x = m(hdr.x - 1 + slot % G::OW, nxo, px);
-    const int y = m(hdr.y - 1 + slot / G::OW, nyo, py);
-    const int z = m(hdr.z - 1 + row, nzo, pz);
-    return (z * nyo + y) * nxo + x;
+    return tab[G::NSLOT + row] + tab[slot];
   }
   __device__ __forceinline__ void init_barriers() {
     if (threadIdx.x == 0) {
