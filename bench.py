@@ -17,6 +17,11 @@ roofline     dominant kernel (godunov_pencil_kernel), algorithmic bytes per
              cell-update (48 B FP32-bulk, 80 B FP64) / CUDA-event kernel time
 cpu_baseline the CPU restatement of the reference path (oracle/, OpenMP over
              oct blocks) timed on this host on one 256^3 step
+batch        the 1024-problem Riemann/blast ensemble (sides 16-128, 50 steps)
+             in one persistent launch per step, FP32-bulk and FP64, tile
+             autotuned on the ensemble
+serve        a Poisson stream of 2D/3D solve requests served with continuous
+             batching; solve_latency_s holds its p50/p99 time-to-solution
 accuracy     density/momentum/energy relative L1 of one FP32-bulk step against
              the FP64 oracle step from the same state
 
@@ -161,6 +166,82 @@ def kernel_time(gpu, steps, dt):
     return gpu.bench_godunov(LEVEL, max(3, steps), dt)
 
 
+def bench_batch(args, rank, world, dist):
+    """The batched ensemble: riemann_blast_ensemble(args.batch_problems) split
+    over the ranks (whole problems per GPU, no exchange), tile autotuned on the
+    ensemble itself, then ``args.batch_steps`` steps of every problem timed
+    with CUDA events (graph replays).  Returns per-precision results with the
+    max-over-ranks time and the whole-job cell-updates/s."""
+    from ramses2_b200.batch import Batch, ensemble_octs, riemann_blast_ensemble
+
+    ens_all = riemann_blast_ensemble(args.batch_problems, steps=args.batch_steps)
+    ens = ens_all[rank::world]
+    noct = ensemble_octs(ens)
+    out = {"workload": "%d independent 3D Riemann/blast problems, sides in {16..128}, %d steps each, HLLC, "
+                       "moncen, split over %d GPU(s)" % (len(ens_all), args.batch_steps, world),
+           "cells": ensemble_octs(ens_all) * 8}
+    for prec in ("fp32_bulk", "fp64"):
+        b = Batch(prec, slope_type=2, riemann="hllc", pool_octs=noct + 64, device=int(os.environ.get("LOCAL_RANK", 0)))
+        for p, ic in ens:
+            p.max_steps = 1 << 30
+            b.add(p, ic)
+        best, _ = b.tune()
+        for pid in list(b.problems):
+            b.remove(pid)
+        for p, ic in ens:
+            p.max_steps = args.batch_steps
+            b.add(p, ic)
+        if dist is not None:
+            dist.barrier()
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+            ms = b.bench(args.batch_steps)
+        done, nstep, _ = b.poll()
+        ok = bool(done[:len(ens)].all() and (nstep[:len(ens)] == args.batch_steps).all())
+        b.close()
+        if dist is not None:
+            import torch
+
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        out[prec] = {"value": out["cells"] / (ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms,
+                     "tile": best, "all_problems_finished": ok, "clocks": clk.summary()}
+    out["fp32_bulk_over_fp64"] = out["fp64"]["ms_per_step"] / out["fp32_bulk"]["ms_per_step"]
+    return out
+
+
+def bench_serve(args, rank, world, dist):
+    """A serving session per GPU: make_requests(args.serve_requests) arriving
+    as a Poisson stream at args.serve_rate per second (own seed per rank),
+    continuous batching over a 16 GiB pool.  Reports time-to-solution
+    percentiles (rank 0's stream) and whole-job cell-updates/s."""
+    from ramses2_b200.serve import HydroServer, make_requests
+
+    out = {"workload": "%d requests per GPU at %.1f/s: 2D 64^2-1024^2 Sedov/interfaces and 3D 32^3-192^3 "
+                       "Sedov (E in [0.1,10]), 20-400 steps each, HLLC, moncen" % (args.serve_requests,
+                                                                                  args.serve_rate)}
+    for prec in ("fp32_bulk", "fp64"):
+        srv = HydroServer(prec, pool_bytes=16 << 30, chunk=4, keep_results=False)
+        srv.run(make_requests(4, rate_hz=1e6, seed=1, steps=(4, 8)), realtime=False)  # warm-up
+        reqs = make_requests(args.serve_requests, rate_hz=args.serve_rate, seed=20261203 + rank)
+        if dist is not None:
+            dist.barrier()
+        st = srv.run(reqs, realtime=True)
+        srv.close()
+        if dist is not None:
+            import torch
+
+            t = torch.tensor([float(st["cell_updates"]), st["makespan_s"]], device="cuda", dtype=torch.float64)
+            upd = t[:1].clone()
+            dist.all_reduce(upd, op=dist.ReduceOp.SUM)
+            mk = t[1:].clone()
+            dist.all_reduce(mk, op=dist.ReduceOp.MAX)
+            st["cell_updates"], st["makespan_s"] = float(upd.item()), float(mk.item())
+            st["cell_updates_per_s"] = st["cell_updates"] / st["makespan_s"]
+        out[prec] = st
+    return out
+
+
 def run_ours(args):
     import ctypes as C
 
@@ -225,6 +306,8 @@ def run_ours(args):
             results["e2e_ms"] = e2e_ms.value / args.steps
             results["e2e_bytes"] = int(m.uold.nbytes)
         gpu.close()
+    batch = bench_batch(args, rank, world, dist) if args.batch_problems > 0 else None
+    serve = bench_serve(args, rank, world, dist) if args.serve_requests > 0 else None
     # max over ranks
     if dist is not None:
         import torch
@@ -323,6 +406,10 @@ def run_ours(args):
                      "bytes_per_cell_update": B_ALG[prec]},
         "cpu_baseline": cpu,
         "accuracy": acc,
+        "solve_latency_s": None if serve is None else {
+            p: {"p50": serve[p]["latency_p50_s"], "p99": serve[p]["latency_p99_s"]} for p in ("fp32_bulk", "fp64")},
+        "batch": batch,
+        "serve": serve,
         "gpu_launches": launches,
         "clocks": results[prec]["clocks"],
     }
@@ -382,6 +469,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / accuracy leg")
     ap.add_argument("--acc-steps", type=int, default=100, help="steps before the accuracy comparison")
+    ap.add_argument("--batch-problems", type=int, default=1024, help="batched ensemble size (0: skip)")
+    ap.add_argument("--batch-steps", type=int, default=50)
+    ap.add_argument("--serve-requests", type=int, default=60, help="serving session length (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="request arrivals per second")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
