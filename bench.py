@@ -174,8 +174,10 @@ def bench_batch(args, rank, world, dist):
     max-over-ranks time and the whole-job cell-updates/s."""
     from ramses2_b200.batch import Batch, ensemble_octs, riemann_blast_ensemble
 
+    from ramses2_b200.ranks import max_over_ranks, shard
+
     ens_all = riemann_blast_ensemble(args.batch_problems, steps=args.batch_steps)
-    ens = ens_all[rank::world]
+    ens = shard(ens_all, rank, world)
     noct = ensemble_octs(ens)
     out = {"workload": "%d independent 3D Riemann/blast problems, sides in {16..128}, %d steps each, HLLC, "
                        "moncen, split over %d GPU(s)" % (len(ens_all), args.batch_steps, world),
@@ -198,12 +200,7 @@ def bench_batch(args, rank, world, dist):
         done, nstep, _ = b.poll()
         ok = bool(done[:len(ens)].all() and (nstep[:len(ens)] == args.batch_steps).all())
         b.close()
-        if dist is not None:
-            import torch
-
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks([ms], dist)[0]
         out[prec] = {"value": out["cells"] / (ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms,
                      "tile": best, "all_problems_finished": ok, "clocks": clk.summary()}
     out["fp32_bulk_over_fp64"] = out["fp64"]["ms_per_step"] / out["fp32_bulk"]["ms_per_step"]
@@ -215,6 +212,7 @@ def bench_serve(args, rank, world, dist):
     as a Poisson stream at args.serve_rate per second (own seed per rank),
     continuous batching over a 16 GiB pool.  Reports time-to-solution
     percentiles (rank 0's stream) and whole-job cell-updates/s."""
+    from ramses2_b200.ranks import max_over_ranks, sum_over_ranks
     from ramses2_b200.serve import HydroServer, make_requests
 
     out = {"workload": "%d requests per GPU at %.1f/s: 2D 64^2-1024^2 Sedov/interfaces and 3D 32^3-192^3 "
@@ -229,14 +227,8 @@ def bench_serve(args, rank, world, dist):
         st = srv.run(reqs, realtime=True)
         srv.close()
         if dist is not None:
-            import torch
-
-            t = torch.tensor([float(st["cell_updates"]), st["makespan_s"]], device="cuda", dtype=torch.float64)
-            upd = t[:1].clone()
-            dist.all_reduce(upd, op=dist.ReduceOp.SUM)
-            mk = t[1:].clone()
-            dist.all_reduce(mk, op=dist.ReduceOp.MAX)
-            st["cell_updates"], st["makespan_s"] = float(upd.item()), float(mk.item())
+            st["cell_updates"] = sum_over_ranks([st["cell_updates"]], dist)[0]
+            st["makespan_s"] = max_over_ranks([st["makespan_s"]], dist)[0]
             st["cell_updates_per_s"] = st["cell_updates"] / st["makespan_s"]
         out[prec] = st
     return out
@@ -310,12 +302,10 @@ def run_ours(args):
     serve = bench_serve(args, rank, world, dist) if args.serve_requests > 0 else None
     # max over ranks
     if dist is not None:
-        import torch
+        from ramses2_b200.ranks import max_over_ranks
 
-        t = torch.tensor([results["fp32_bulk"]["ms_per_step"], results["fp64"]["ms_per_step"],
-                          results["e2e_ms"]], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        results["fp32_bulk"]["ms_per_step"], results["fp64"]["ms_per_step"], results["e2e_ms"] = t.tolist()
+        results["fp32_bulk"]["ms_per_step"], results["fp64"]["ms_per_step"], results["e2e_ms"] = max_over_ranks(
+            [results["fp32_bulk"]["ms_per_step"], results["fp64"]["ms_per_step"], results["e2e_ms"]], dist)
     if rank != 0:
         if dist is not None:
             dist.barrier()
