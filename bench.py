@@ -234,6 +234,128 @@ def bench_serve(args, rank, world, dist):
     return out
 
 
+def _timed(L, fn):
+    """Device time of fn() (CUDA events on the library stream), ms."""
+    import ctypes as C
+
+    from ramses2_b200._lib import check
+
+    ms = C.c_float()
+    check(L.rh_timer_start(), "rh_timer_start")
+    fn()
+    check(L.rh_timer_stop(C.byref(ms)), "rh_timer_stop")
+    return ms.value
+
+
+def leaf_rel_l1(m, a, b):
+    """Relative L1 (rho, mx, my, mz, E) over the leaf cells of every level."""
+    num = np.zeros(5)
+    den = np.zeros(5)
+    for lev in range(m.levelmin, m.levelmax + 1):
+        if not m.noct[lev]:
+            continue
+        sl = m.level_slice(lev)
+        leaf = m.leaf_mask(lev)[:, None, :]
+        num += (np.abs(a[sl] - b[sl]) * leaf).sum(axis=(0, 2))
+        den += (np.abs(b[sl]) * leaf).sum(axis=(0, 2))
+    return dict(zip(["rho", "mx", "my", "mz", "E"], (num / np.where(den > 0, den, 1.0)).tolist()))
+
+
+def bench_amr(args, rank, world, dist, device):
+    """Config-1 style AMR Sedov: levels 7-10 refined by hydro_refine's 0.1
+    density/pressure gradient criterion on a developed Sedov-like blast
+    (2-6 M leaf cells), HLLC, moncen, Courant 0.8, coarse steps with
+    nsubcycle=1 (courant_fine of every level, then every level's Godunov
+    step).  FP64 and FP32-bulk timed over args.amr_steps steps; FP32-bulk
+    relative L1 against FP64 (leaf cells) after every step of the FP64
+    trajectory (same dt sequence)."""
+    from ramses2_b200._abi import HydroParams
+    from ramses2_b200._lib import lib
+    from ramses2_b200.hydro import GodunovGPU, amr_coarse_step
+    from ramses2_b200.mesh import sedov_amr_mesh
+    from ramses2_b200.ranks import max_over_ranks
+
+    m, g = sedov_amr_mesh(7, 10, radius=0.08)
+    P = HydroParams.make(gamma=g, courant_factor=0.8, slope_type=2, riemann="hllc", interpol_var=0,
+                         interpol_type=1)
+    L = lib()
+    u0 = m.uold.copy()
+    leaf = m.ncells_leaf()
+    allcells = int(m.noct_total) * 8
+    out = {"workload": "AMR Sedov, levels 7-10, hydro_refine err_grad_d = err_grad_p = 0.1 on a developed blast",
+           "leaf_cells": leaf, "cells_all_levels": allcells,
+           "octs_per_level": {str(l): int(m.noct[l]) for l in range(7, 11)}, "steps": args.amr_steps}
+    fp64_traj = None
+    for prec in ("fp64", "fp32_bulk"):
+        m.uold[:] = u0
+        gpu = GodunovGPU(m, P, precision=prec, device=device)
+        for _ in range(2):
+            amr_coarse_step(gpu, m)
+        gpu.push_uold(u0)
+        per, dts, states = [], [], []
+        for _ in range(args.amr_steps):
+            res = {}
+            per.append(_timed(L, lambda: res.__setitem__("dt", amr_coarse_step(gpu, m))))
+            dts.append(res["dt"])
+            if prec == "fp64":
+                states.append(gpu.fetch_uold())
+        if prec == "fp64":
+            fp64_traj = (dts, states)
+        else:
+            # accuracy along the FP64 trajectory: same dt sequence, untimed
+            gpu.push_uold(u0)
+            errs = []
+            for dt, ref in zip(*fp64_traj):
+                amr_coarse_step(gpu, m, dt)
+                errs.append(leaf_rel_l1(m, gpu.fetch_uold(), ref))
+            out["fp32_bulk_vs_fp64_rel_l1_per_step"] = errs
+        gpu.close()
+        ms = max_over_ranks([float(np.mean(per))], dist)[0]
+        out[prec] = {"value": world * leaf / (ms * 1e-3), "unit": "leaf cell-updates/s", "ms_per_coarse_step": ms,
+                     "all_level_cell_updates_per_s": world * allcells / (ms * 1e-3),
+                     "ms_each_step": [round(v, 3) for v in per]}
+    out["fp32_bulk_over_fp64"] = out["fp64"]["ms_per_coarse_step"] / out["fp32_bulk"]["ms_per_coarse_step"]
+    out["density_l1_le_1e-5"] = bool(all(e["rho"] <= 1e-5 for e in out["fp32_bulk_vs_fp64_rel_l1_per_step"]))
+    out["_mesh"] = (m, P, u0)
+    return out
+
+
+def bench_turbulence(args, rank, world, dist, device):
+    """Config-2: decaying supersonic turbulence on 256^3 (gamma 1.001, rms
+    Mach 5, lognormal density, minmod, HLLC, periodic), args.turb_steps
+    FP32-bulk and FP64 steps; FP32-bulk relative L1 against FP64 after them."""
+    from ramses2_b200._abi import HydroParams
+    from ramses2_b200._lib import lib
+    from ramses2_b200.hydro import GodunovGPU
+    from ramses2_b200.mesh import turbulence3d, uniform_mesh
+    from ramses2_b200.ranks import max_over_ranks
+
+    m = uniform_mesh(LEVEL, nsubgrid=1, bc="periodic")
+    turbulence3d(m, gamma=1.001, mach=5.0)
+    P = HydroParams.make(gamma=1.001, courant_factor=0.8, slope_type=1, riemann="hllc")
+    L = lib()
+    u0 = m.uold.copy()
+    ncell = int(m.noct[LEVEL]) * 8
+    out = {"workload": "decaying turbulence 256^3, gamma 1.001, rms Mach 5, minmod, HLLC",
+           "cells": ncell, "steps": args.turb_steps}
+    final = {}
+    for prec in ("fp64", "fp32_bulk"):
+        m.uold[:] = u0
+        gpu = GodunovGPU(m, P, precision=prec, device=device)
+        gpu.step_uniform()
+        gpu.push_uold(u0)
+        ms = _timed(L, lambda: [gpu.step_uniform() for _ in range(args.turb_steps)]) / args.turb_steps
+        final[prec] = gpu.fetch_uold()
+        gpu.close()
+        ms = max_over_ranks([ms], dist)[0]
+        out[prec] = {"value": world * ncell / (ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms}
+    out["fp32_bulk_over_fp64"] = out["fp64"]["ms_per_step"] / out["fp32_bulk"]["ms_per_step"]
+    names = ["rho", "mx", "my", "mz", "E"]
+    out["fp32_bulk_vs_fp64_rel_l1_after_steps"] = dict(zip(names, rel_l1(final["fp32_bulk"], final["fp64"])))
+    out["_state"] = (m, P, final["fp64"])
+    return out
+
+
 def run_ours(args):
     import ctypes as C
 
@@ -298,6 +420,8 @@ def run_ours(args):
             results["e2e_ms"] = e2e_ms.value / args.steps
             results["e2e_bytes"] = int(m.uold.nbytes)
         gpu.close()
+    amr = bench_amr(args, rank, world, dist, device) if args.amr_steps > 0 else None
+    turb = bench_turbulence(args, rank, world, dist, device) if args.turb_steps > 0 else None
     batch = bench_batch(args, rank, world, dist) if args.batch_problems > 0 else None
     serve = bench_serve(args, rank, world, dist) if args.serve_requests > 0 else None
     # max over ranks
@@ -355,6 +479,39 @@ def run_ours(args):
                "cumulative_steps": args.acc_steps}
         acc["density_l1_le_1e-5"] = bool(acc["per_step_fp32_bulk_vs_fp64_oracle_rel_l1"]["rho"] <= 1e-5 and
                                          acc["cumulative_fp32_bulk_vs_fp64_rel_l1"]["rho"] <= 1e-5)
+        # one step of each precision against the oracle on the AMR and turbulence states
+        from ramses2_b200.hydro import amr_coarse_step
+
+        if amr is not None:
+            ma, Pa, ua = amr.pop("_mesh")
+            ma.uold[:] = ua
+            oa = oracle.OracleHydro(ma, Pa, nthreads=nthreads)
+            dta = amr_coarse_step(oa, ma)
+            refa = ma.uold.copy()
+            amr["one_step_vs_oracle_rel_l1"] = {}
+            for prec in ("fp64", "fp32_bulk"):
+                ma.uold[:] = ua
+                gpu = GodunovGPU(ma, Pa, precision=prec, device=device)
+                amr_coarse_step(gpu, ma, dta)
+                amr["one_step_vs_oracle_rel_l1"][prec] = leaf_rel_l1(ma, gpu.fetch_uold(), refa)
+                gpu.close()
+        if turb is not None:
+            mt, Pt, st = turb.pop("_state")
+            mt.uold[:] = st
+            ot = oracle.OracleHydro(mt, Pt, nthreads=nthreads)
+            dtt, _ = ot.step_uniform()
+            reft = mt.uold.copy()
+            turb["one_step_vs_oracle_rel_l1"] = {}
+            for prec in ("fp64", "fp32_bulk"):
+                mt.uold[:] = st
+                gpu = GodunovGPU(mt, Pt, precision=prec, device=device)
+                gpu.step_uniform(dtt)
+                turb["one_step_vs_oracle_rel_l1"][prec] = dict(zip(names, rel_l1(gpu.fetch_uold(), reft)))
+                gpu.close()
+    if amr is not None:
+        amr.pop("_mesh", None)
+    if turb is not None:
+        turb.pop("_state", None)
     peak, peak_kind = measured_peaks()
     prec = "fp32_bulk"
     ms = results[prec]["ms_per_step"]
@@ -398,6 +555,8 @@ def run_ours(args):
         "accuracy": acc,
         "solve_latency_s": None if serve is None else {
             p: {"p50": serve[p]["latency_p50_s"], "p99": serve[p]["latency_p99_s"]} for p in ("fp32_bulk", "fp64")},
+        "amr": amr,
+        "turbulence": turb,
         "batch": batch,
         "serve": serve,
         "gpu_launches": launches,
@@ -459,6 +618,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / accuracy leg")
     ap.add_argument("--acc-steps", type=int, default=100, help="steps before the accuracy comparison")
+    ap.add_argument("--amr-steps", type=int, default=10, help="AMR Sedov coarse steps (0: skip)")
+    ap.add_argument("--turb-steps", type=int, default=100, help="turbulence 256^3 steps (0: skip)")
     ap.add_argument("--batch-problems", type=int, default=1024, help="batched ensemble size (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=50)
     ap.add_argument("--serve-requests", type=int, default=60, help="serving session length (0: skip)")

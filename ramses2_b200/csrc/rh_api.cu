@@ -111,14 +111,15 @@ template <typename E> __global__ void copy_kernel(E* __restrict__ dst, const E* 
 // per-block partial (mass, ekin, eint, emag, dt).  hydro/courant_fine.f90:57-168
 __global__ void cmpdt_kernel(const double* __restrict__ ud, const float* __restrict__ uf, int fp32,
                              const uint8_t* __restrict__ refined, long long oct0, long long noct, CflConst C,
-                             double vol, double* __restrict__ partial) {
+                             double vol, double* __restrict__ partial, const uint8_t* __restrict__ refbits) {
   __shared__ double red[32][4];
   long long cell_id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double m = 0, ek = 0, ei = 0, dt = 1e300;
   if (cell_id < noct * 8) {
     long long oct = oct0 + cell_id / 8;
     int cell = (int)(cell_id % 8);
-    if (!refined || !refined[cell_id]) {
+    const bool ref = refined ? refined[cell_id] != 0 : (refbits ? ((refbits[oct] >> cell) & 1) != 0 : false);
+    if (!ref) {
       double r, m1, m2, m3, E;
       if (!fp32) {
         const double* o = ud + oct * 40 + cell;
@@ -582,6 +583,7 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
   c.unew_written.assign(c.levelmax + 1, 0);
   c.cfl_on_unew.assign(c.levelmax + 1, 0);
   c.cfl_on_uold.assign(c.levelmax + 1, 0);
+  c.cfl_keys.assign(8 * (c.levelmax + 1), 0.0);
   c.have_mesh = true;
   rc = upload_uold(uold);
   if (rc) return rc;
@@ -746,7 +748,8 @@ int rh_cmpdt(int head_idx, int num_octs, double dx, double gamma, double smallr,
   }
   const int l = level_of_range(head_idx, num_octs);
   const double key[8] = {dx, gamma, smallr, smallc, courant_factor, g[0], g[1], g[2]};
-  const bool same_key = std::equal(key, key + 8, c.cfl_key);
+  double* lkey = l >= 0 ? &c.cfl_keys[8 * l] : nullptr;
+  const bool same_key = lkey && std::equal(key, key + 8, lkey);
   double out[5];
   if (l >= 0 && c.cfl_on_uold[l] && same_key) {
     RH_CUDA(cudaMemcpyAsync(out, c.d_cfl + 5 * l, sizeof out, cudaMemcpyDeviceToHost, c.stream));
@@ -761,34 +764,22 @@ int rh_cmpdt(int head_idx, int num_octs, double dx, double gamma, double smallr,
       RH_CUDA(cudaMalloc(&c.d_scratch, sizeof(double) * 5 * nblk));
       c.scratch_elems = (size_t)nblk * 5;
     }
-    // leaf mask of the level (refined flags of the grid records)
-    std::vector<uint8_t> ref((size_t)num_octs * 8);
-    bool any = false;
-    for (long long i = 0; i < num_octs; ++i)
-      for (int k = 0; k < 8; ++k) {
-        ref[i * 8 + k] = c.grid[head_idx - 1 + i].refined[k] ? 1 : 0;
-        any |= ref[i * 8 + k] != 0;
-      }
-    uint8_t* d_ref = nullptr;
-    if (any) {
-      RH_CUDA(cudaMalloc(&d_ref, ref.size()));
-      RH_CUDA(cudaMemcpyAsync(d_ref, ref.data(), ref.size(), cudaMemcpyHostToDevice, c.stream));
-    }
+    // leaf mask: the refined-cell bits of the grid records, resident since rh_set_mesh
     const CflConst C = make_cfl(dx, gamma, smallr, smallc, courant_factor, g);
     const double vol = dx * dx * dx;
     const bool fp32 = c.precision == RH_PREC_FP32_BULK;
-    cmpdt_kernel<<<(unsigned)nblk, threads, 0, c.stream>>>(c.ud[c.cur], c.uf[c.cur], fp32 ? 1 : 0, d_ref,
-                                                           head_idx - 1, num_octs, C, vol, c.d_scratch);
+    cmpdt_kernel<<<(unsigned)nblk, threads, 0, c.stream>>>(c.ud[c.cur], c.uf[c.cur], fp32 ? 1 : 0, nullptr,
+                                                           head_idx - 1, num_octs, C, vol, c.d_scratch,
+                                                           c.d_refmask);
     RH_CUDA(cudaGetLastError());
     double* d_out = c.d_cfl + 5 * (l >= 0 ? l : 0);
     reduce_partials_kernel<<<1, 1024, 0, c.stream>>>(c.d_scratch, nblk, 1e300, d_out);
     RH_CUDA(cudaGetLastError());
     RH_CUDA(cudaMemcpyAsync(out, d_out, sizeof out, cudaMemcpyDeviceToHost, c.stream));
     RH_CUDA(cudaStreamSynchronize(c.stream));
-    if (d_ref) cudaFree(d_ref);
     if (l >= 0) c.cfl_on_uold[l] = 0;
   }
-  std::copy(key, key + 8, c.cfl_key);
+  if (lkey) std::copy(key, key + 8, lkey);
   *mass = out[0];
   *ekin = out[1];
   *eint = out[2];
@@ -837,7 +828,8 @@ static int launch_level(int l, double gamma, double smallr, double smallc, doubl
   for (int i = 0; i < 6; ++i) A.btype[i] = c.bound_type[i];
   A.ghost_base = c.ngridmax;
   A.err = c.d_err;
-  const double courant = c.cfl_key[4] > 0 ? c.cfl_key[4] : smax_cap * dt / dx;
+  const double* lkey = &c.cfl_keys[8 * l];
+  const double courant = lkey[4] > 0 ? lkey[4] : smax_cap * dt / dx;
   A.cfl = make_cfl(dx, gamma, smallr, smallc, courant, g);
   A.vol = dx * dx * dx;
   A.cfl_partial = fuse_cfl ? T.d_cfl_partial : nullptr;
@@ -917,9 +909,9 @@ int rh_godunov(int head_idx, int num_subgrids, int ngridmax, int ilevel, int lev
   if (constant_gravity)
     for (int d = 0; d < 3; ++d) g[d] = constant_gravity[d];
   // The fused CFL epilogue uses the parameters of the last rh_cmpdt call.
-  const bool fuse = c.cfl_key[0] == dx && c.cfl_key[1] == gamma && c.cfl_key[2] == smallr &&
-                    c.cfl_key[5] == g[0] && c.cfl_key[6] == g[1] && c.cfl_key[7] == g[2] &&
-                    c.cfl_key[3] * c.cfl_key[3] == smallc2;
+  const double* key = &c.cfl_keys[8 * l];
+  const bool fuse = key[0] == dx && key[1] == gamma && key[2] == smallr && key[5] == g[0] && key[6] == g[1] &&
+                    key[7] == g[2] && key[3] * key[3] == smallc2;
   rc = launch_level(l, gamma, smallr, std::sqrt(smallc2), dt, dx, smax_cap, slope, riemann, g, fuse,
                     c.unew_copied[l] != 0);
   if (rc) return rc;

@@ -89,7 +89,7 @@ struct Context {
   std::vector<char> unew_written;  // godunov wrote unew for the whole level
   std::vector<char> cfl_on_unew;   // d_cfl[l] holds CFL values of unew
   std::vector<char> cfl_on_uold;   // d_cfl[l] holds CFL values of uold
-  double cfl_key[8] = {0};         // parameters the cached CFL values were computed with
+  std::vector<double> cfl_keys;    // [levelmax+1][8]: parameters of each level's cached CFL values
   // timing of the last godunov launch (for the bench)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };

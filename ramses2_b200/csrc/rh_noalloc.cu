@@ -20,7 +20,7 @@ namespace rh {
 // Defined in rh_api.cu: per-block courant_fine partials and their reduction.
 __global__ void cmpdt_kernel(const double* __restrict__ ud, const float* __restrict__ uf, int fp32,
                              const uint8_t* __restrict__ refined, long long oct0, long long noct, CflConst C,
-                             double vol, double* __restrict__ partial);
+                             double vol, double* __restrict__ partial, const uint8_t* __restrict__ refbits);
 __global__ void reduce_partials_kernel(const double* __restrict__ partial, long long n, double dt0,
                                        double* __restrict__ out);
 }  // namespace rh
@@ -101,7 +101,7 @@ int rh_cmpdt_noalloc(const double* d_uold, int num_octs, const unsigned char* d_
   const long long nblk = (ncell + kThreads - 1) / kThreads;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   rh::cmpdt_kernel<<<(unsigned)nblk, kThreads, 0, st>>>(d_uold, nullptr, 0, d_refined, 0, num_octs, C,
-                                                         dx * dx * dx, scratch);
+                                                         dx * dx * dx, scratch, nullptr);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return rh::cuda_fail(e, "cmpdt_kernel (noalloc)");
   rh::reduce_partials_kernel<<<1, 1024, 0, st>>>(scratch, nblk, dx / smallc, d_out);

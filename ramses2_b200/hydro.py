@@ -116,3 +116,22 @@ class GodunovGPU:
 
     def close(self):
         check(self.L.rh_finalize(), "rh_finalize")
+
+
+def amr_coarse_step(solver, mesh, dt=None):
+    """One coarse step of every level with nsubcycle = 1, in amr/amr_step.f90's
+    order: courant_fine of every level (the smallest dt wins,
+    amr/amr_step.f90:588), set_unew coarse to fine, then godunov_fine and
+    set_uold from the finest level to the coarsest (the coarse update of level
+    l lands in unew of level l-1 before that level is stepped).  ``solver`` is
+    a :class:`GodunovGPU` (or anything with the same four leaf calls)."""
+    lev = [l for l in range(mesh.levelmin, mesh.levelmax + 1) if mesh.noct[l]]
+    if dt is None:
+        dt = min(min(mesh.dx(l) / solver.params.smallc, solver.courant_fine(l)[4]) for l in lev)
+    for l in lev:
+        solver.set_unew(l)
+    for l in reversed(lev):
+        solver.godunov_fine(l, dt)
+        solver.set_uold(l)
+    return dt
+

@@ -272,12 +272,24 @@ def riemann3d_state(rng, n_cells, gamma=None):
 # ---------------------------------------------------------------------------
 # Static AMR meshes
 # ---------------------------------------------------------------------------
-def _dilate_keys(keys, r):
-    """All integer points within Chebyshev distance r of the given (n,3) keys."""
-    offs = np.array([(i, j, k) for i in range(-r, r + 1) for j in range(-r, r + 1) for k in range(-r, r + 1)],
-                    dtype=np.int64)
-    out = (keys[:, None, :] + offs[None, :, :]).reshape(-1, 3)
-    return np.unique(out, axis=0)
+def _shift_reduce(a, r, op, fill):
+    """Separable Chebyshev-window reduction (op = np.logical_or / logical_and)
+    of a dense boolean grid over offsets -r..r per axis; outside the grid
+    counts as ``fill``."""
+    out = a
+    for ax in range(a.ndim):
+        pad = [(0, 0)] * a.ndim
+        pad[ax] = (r, r)
+        p = np.pad(out, pad, constant_values=fill)
+        acc = None
+        n = out.shape[ax]
+        for k in range(2 * r + 1):
+            sl = [slice(None)] * a.ndim
+            sl[ax] = slice(k, k + n)
+            v = p[tuple(sl)]
+            acc = v.copy() if acc is None else op(acc, v, out=acc)
+        out = acc
+    return out
 
 
 def amr_mesh(levelmin, levelmax, refine, bc="outflow", boxlen=1.0, nexpand=1, box_nx=(1, 1, 1)):
@@ -290,11 +302,11 @@ def amr_mesh(levelmin, levelmax, refine, bc="outflow", boxlen=1.0, nexpand=1, bo
     interpolating a missing fine neighbour needs (father cell and its six
     neighbours, hydro/interpol_hydro.f90:5-109).  Out-of-box neighbours do not
     count against the margin.  Octs are stored level by level in Morton order,
-    and ``refined`` flags mark the cells that have children.
+    and ``refined`` flags mark the cells that have children.  Works on dense
+    boolean grids of each level's cells (one byte per cell of the level's box).
     """
     nb = np.array(box_nx, dtype=np.int64)
     levels = {}
-    # level levelmin: all octs
     no = nb << (levelmin - 1)
     ix, iy, iz = np.meshgrid(np.arange(no[0]), np.arange(no[1]), np.arange(no[2]), indexing="ij")
     levels[levelmin] = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], axis=1).astype(np.int64)
@@ -302,29 +314,23 @@ def amr_mesh(levelmin, levelmax, refine, bc="outflow", boxlen=1.0, nexpand=1, bo
         octs = levels[l]
         cells = (2 * octs[:, None, :] + CELL_OFF[None, :, :]).reshape(-1, 3)
         dx = boxlen / 2.0 ** l
-        flag = refine((cells + 0.5) * dx, l)
-        fk = cells[flag]
-        if len(fk) == 0:
+        flag = np.asarray(refine((cells + 0.5) * dx, l), dtype=bool)
+        if not flag.any():
             break
+        ncell = tuple(int(v) for v in (nb << l))
+        F = np.zeros(ncell, dtype=bool)
+        fc = cells[flag]
+        F[fc[:, 0], fc[:, 1], fc[:, 2]] = True
         if nexpand > 0:
-            fk = _dilate_keys(fk, nexpand)
-        ncell = nb << l
-        inbox = np.all((fk >= 0) & (fk < ncell[None, :]), axis=1)
-        fk = fk[inbox]
-        # margin: every cell within 2 of a flagged cell (inside the box) must exist at level l
-        covered = set(map(tuple, cells.tolist()))
-        ok = np.ones(len(fk), dtype=bool)
-        offs = [(i, j, k) for i in range(-2, 3) for j in range(-2, 3) for k in range(-2, 3)]
-        for n, c in enumerate(fk.tolist()):
-            for o in offs:
-                q = (c[0] + o[0], c[1] + o[1], c[2] + o[2])
-                if all(0 <= q[d] < ncell[d] for d in range(3)) and q not in covered:
-                    ok[n] = False
-                    break
-        fk = fk[ok]
+            F = _shift_reduce(F, nexpand, np.logical_or, False)
+        cov = np.zeros(ncell, dtype=bool)
+        cov[cells[:, 0], cells[:, 1], cells[:, 2]] = True
+        # margin: every in-box cell within 2 of a candidate must exist at level l
+        F &= _shift_reduce(cov, 2, np.logical_and, True)
+        fk = np.argwhere(F).astype(np.int64)
         if len(fk) == 0:
             break
-        levels[l + 1] = np.unique(fk, axis=0)  # child oct keys at level l+1 = flagged cell coords
+        levels[l + 1] = fk  # child oct keys at level l+1 = flagged cell coords (lexicographic)
     lmax = max(levels)
     grids = []
     for l in range(levelmin, lmax + 1):
@@ -337,10 +343,12 @@ def amr_mesh(levelmin, levelmax, refine, bc="outflow", boxlen=1.0, nexpand=1, bo
         g["lev"] = l
         g["hkey"] = _morton3(k[:, 0], k[:, 1], k[:, 2])
         if l < lmax:
-            child = set(map(tuple, levels[l + 1].tolist())) if (l + 1) in levels else set()
-            cells = (2 * k[:, None, :] + CELL_OFF[None, :, :])
-            ref = np.array([[tuple(c) in child for c in oc] for oc in cells.tolist()], dtype=np.uint8)
-            g["refined"] = ref
+            ncell = tuple(int(v) for v in (nb << l))
+            ch = np.zeros(ncell, dtype=bool)
+            kc = levels[l + 1]
+            ch[kc[:, 0], kc[:, 1], kc[:, 2]] = True
+            cells = 2 * k[:, None, :] + CELL_OFF[None, :, :]
+            g["refined"] = ch[cells[..., 0], cells[..., 1], cells[..., 2]].astype(np.uint8)
         grids.append(g)
     grid = np.concatenate(grids)
     return Mesh(grid, levelmin, lmax, nsubgrid=1, boxlen=boxlen, bc=bc, box_nx=box_nx)
@@ -354,3 +362,66 @@ def fill_amr_prim(mesh, prim_fn, gamma):
         x = mesh.cell_centres(lev)
         rho, u, v, w, p = prim_fn(x, lev)
         set_level_prim(mesh, lev, rho, u, v, w, p, gamma)
+
+
+# ---------------------------------------------------------------------------
+# Gradient refinement criterion and a developed Sedov-like blast (config 1)
+# ---------------------------------------------------------------------------
+def hydro_refine_flags(prim_fn, x, dx, err_grad_d=0.1, err_grad_p=0.1, floor_d=1e-10, floor_p=1e-10):
+    """hydro_refine's density and pressure criteria (hydro/godunov_utils.f90:
+    6-223): a cell is flagged when, along some axis, 2 max(|d_r - d|/(d_r + d
+    + floor), |d - d_l|/(d + d_l + floor)) exceeds err_grad (same for p), with
+    the left/right neighbours at x -+ dx.  ``prim_fn(x) -> (rho, u, v, w, p)``."""
+    rho, _, _, _, p = prim_fn(x)
+    ok = np.zeros(x.shape[:-1], dtype=bool)
+    for d in range(3):
+        e = np.zeros(3)
+        e[d] = dx
+        rl, _, _, _, pl = prim_fn(x - e)
+        rr, _, _, _, pr = prim_fn(x + e)
+        ed = 2.0 * np.maximum(np.abs((rr - rho) / (rr + rho + floor_d)), np.abs((rho - rl) / (rho + rl + floor_d)))
+        ep = 2.0 * np.maximum(np.abs((pr - p) / (pr + p + floor_p)), np.abs((p - pl) / (p + pl + floor_p)))
+        ok |= (ed > err_grad_d) | (ep > err_grad_p)
+    return ok
+
+
+def sedov_like_blast(radius=0.2, gamma=1.4, energy=1.0, rho0=1.0, p0=1e-5, centre=(0.5, 0.5, 0.5), rho_floor=1e-3):
+    """Primitive state of a developed point blast with its shock at ``radius``:
+    strong-shock jump conditions at the front, a steep density profile
+    rho ~ (r/R)^(3/(gamma-1)) behind it, velocity linear in r and a pressure
+    plateau at 30 % of the post-shock value (a closed-form stand-in for the
+    self-similar Sedov-Taylor profile).  Returns prim_fn(x) -> (rho, u, v, w, p)."""
+    xi = 1.15  # Sedov constant for gamma = 1.4 in 3D
+    t = np.sqrt(radius ** 5 * rho0 / (xi ** 5 * energy))
+    rdot = 0.4 * radius / t
+    rho1 = rho0 * (gamma + 1) / (gamma - 1)
+    v1 = 2.0 / (gamma + 1) * rdot
+    p1 = 2.0 / (gamma + 1) * rho0 * rdot ** 2
+    c = np.asarray(centre, dtype=np.float64)
+
+    def prim(x):
+        dxv = x - c
+        r = np.sqrt((dxv ** 2).sum(-1))
+        s = np.minimum(r / radius, 1.0)
+        inside = r < radius
+        rho = np.where(inside, np.maximum(rho1 * s ** (3.0 / (gamma - 1)), rho_floor), rho0)
+        vr = np.where(inside, v1 * s, 0.0)
+        p = np.where(inside, p1 * (0.3 + 0.7 * s ** 8), p0)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            nvec = np.where(r[..., None] > 0, dxv / np.maximum(r, 1e-300)[..., None], 0.0)
+        return rho, vr * nvec[..., 0], vr * nvec[..., 1], vr * nvec[..., 2], p
+
+    return prim
+
+
+def sedov_amr_mesh(levelmin=7, levelmax=10, radius=0.2, gamma=1.4, err_grad=0.1, bc="outflow"):
+    """Config-1 style mesh: levels levelmin..levelmax refined where
+    hydro_refine's relative density/pressure gradient exceeds ``err_grad`` on
+    a developed Sedov-like blast (:func:`sedov_like_blast`), filled with that
+    state.  Returns (mesh, gamma)."""
+    prim = sedov_like_blast(radius=radius, gamma=gamma)
+    m = amr_mesh(levelmin, levelmax,
+                 lambda x, l: hydro_refine_flags(prim, x, 1.0 / 2 ** l, err_grad, err_grad), bc=bc)
+    fill_amr_prim(m, lambda x, l: prim(x), gamma)
+    return m, gamma
+

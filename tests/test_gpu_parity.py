@@ -11,7 +11,7 @@ import pytest
 
 import oracle
 from ramses2_b200._abi import HydroParams
-from ramses2_b200.hydro import GodunovGPU
+from ramses2_b200.hydro import GodunovGPU, amr_coarse_step
 from ramses2_b200.mesh import riemann3d_state, sedov3d, turbulence3d, uniform_mesh
 
 pytestmark = pytest.mark.gpu
@@ -132,6 +132,39 @@ def test_sedov_multistep_fp64():
         gpu.close()
 
 
+def test_config0_sedov64_per_step_over_100_steps():
+    """Config 0 as specified: Sedov 64^3 (levelmin = levelmax = 6, outflow,
+    gamma 1.4, E = 1 within 2 cells, moncen, HLLC, C = 0.8), 100 steps.  Each
+    step the GPU starts from the oracle's state (rh_set_grid_device) and takes
+    the oracle's dt: relative L1 <= 1e-12 per variable at every step.  The
+    GPU's own 100-step trajectory ends within 1e-9 of the oracle's."""
+    m = uniform_mesh(6, nsubgrid=1, bc="outflow")
+    sedov3d(m)
+    P = HydroParams.make(gamma=1.4, courant_factor=0.8, slope_type=2, riemann="hllc")
+    u0 = m.uold.copy()
+    mo = uniform_mesh(6, nsubgrid=1, bc="outflow")
+    mo.uold[:] = u0
+    o = oracle.OracleHydro(mo, P, nthreads=NTHREADS)
+    gpu = GodunovGPU(m, P)
+    worst = np.zeros(5)
+    try:
+        for step in range(100):
+            gpu.push_uold(mo.uold)
+            dto, _ = o.step_uniform()
+            gpu.step_uniform(dto)
+            err = rel_l1(gpu.fetch_uold(), mo.uold)
+            worst = np.maximum(worst, err)
+            assert np.all(err <= TOL_FP64), (step, err)
+        final_oracle = mo.uold.copy()
+        gpu.push_uold(u0)
+        for _ in range(100):
+            gpu.step_uniform()
+        err = rel_l1(gpu.fetch_uold(), final_oracle)
+        assert np.all(err <= 1e-9), err
+    finally:
+        gpu.close()
+
+
 def test_turbulence_one_step_fp64():
     m = uniform_mesh(5, nsubgrid=1, bc="periodic")
     turbulence3d(m, gamma=1.001, mach=5.0)
@@ -184,18 +217,7 @@ def amr_case(bc="outflow", itype=1, ivar=0):
 
 
 def amr_step(solver, m, dt=None):
-    """One coarse step with nsubcycle=1 in amr_step.f90's order: CFL of every
-    level (the finest dt wins, amr_step.f90:588), set_unew coarse to fine, then
-    godunov + set_uold fine to coarse."""
-    lev = [l for l in range(m.levelmin, m.levelmax + 1) if m.noct[l]]
-    if dt is None:
-        dt = min(min(m.dx(l) / solver.params.smallc, solver.courant_fine(l)[4]) for l in lev)
-    for l in lev:
-        solver.set_unew(l)
-    for l in reversed(lev):
-        solver.godunov_fine(l, dt)
-        solver.set_uold(l)
-    return dt
+    return amr_coarse_step(solver, m, dt)
 
 
 @pytest.mark.parametrize("bc,itype,ivar", [("outflow", 1, 0), ("periodic", 2, 1), ("reflexive", 0, 0),
