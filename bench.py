@@ -320,6 +320,43 @@ def bench_amr(args, rank, world, dist, device):
     return out
 
 
+PUBLISHED_512 = {"fp64": 4456e6, "fp32_bulk": 10093e6}  # reference B200, hydro double/single NSUBGRID=4
+
+
+def bench_sedov512(args, rank, world, dist, device, tuned):
+    """The reference's own published configuration: periodic Sedov3D 512^3,
+    HLLC, moncen, whole hydro step (CFL, set_unew, Godunov, set_uold), with
+    the tiles tuned on 256^3.  Reported next to the reference's published
+    B200 figures for that setup (hydro double / single, NSUBGRID=4; the
+    reference's "single" is all-FP32 storage, FP32-bulk keeps E in FP64)."""
+    from ramses2_b200._abi import HydroParams
+    from ramses2_b200._lib import lib
+    from ramses2_b200.hydro import GodunovGPU
+    from ramses2_b200.mesh import sedov3d, uniform_mesh
+    from ramses2_b200.ranks import max_over_ranks
+
+    m = uniform_mesh(9, nsubgrid=1, bc="periodic")
+    sedov3d(m, gamma=1.4, rho0=1.0, p0=1e-5, energy=1.0, radius_cells=2.0)
+    P = HydroParams.make(gamma=1.4, courant_factor=0.8, slope_type=2, riemann="hllc")
+    L = lib()
+    ncell = int(m.noct[9]) * 8
+    out = {"workload": "Sedov3D 512^3 periodic, whole hydro step", "cells": ncell, "steps": args.sedov512_steps}
+    for prec in ("fp64", "fp32_bulk"):
+        gpu = GodunovGPU(m, P, precision=prec, device=device)
+        t = tuned[prec]
+        gpu.set_tile(t["txo"], t["tyo"], t["lz"], t["minb"])
+        for _ in range(3):
+            gpu.step_uniform()
+        ms = _timed(L, lambda: [gpu.step_uniform() for _ in range(args.sedov512_steps)]) / args.sedov512_steps
+        gpu.close()
+        ms = max_over_ranks([ms], dist)[0]
+        v = world * ncell / (ms * 1e-3)
+        out[prec] = {"value": v, "unit": "cell-updates/s", "ms_per_step": ms,
+                     "reference_published_b200": PUBLISHED_512[prec],
+                     "over_reference_published": v / world / PUBLISHED_512[prec]}
+    return out
+
+
 def bench_turbulence(args, rank, world, dist, device):
     """Config-2: decaying supersonic turbulence on 256^3 (gamma 1.001, rms
     Mach 5, lognormal density, minmod, HLLC, periodic), args.turb_steps
@@ -420,6 +457,7 @@ def run_ours(args):
             results["e2e_ms"] = e2e_ms.value / args.steps
             results["e2e_bytes"] = int(m.uold.nbytes)
         gpu.close()
+    s512 = bench_sedov512(args, rank, world, dist, device, tuned) if args.sedov512_steps > 0 else None
     amr = bench_amr(args, rank, world, dist, device) if args.amr_steps > 0 else None
     turb = bench_turbulence(args, rank, world, dist, device) if args.turb_steps > 0 else None
     batch = bench_batch(args, rank, world, dist) if args.batch_problems > 0 else None
@@ -555,6 +593,7 @@ def run_ours(args):
         "accuracy": acc,
         "solve_latency_s": None if serve is None else {
             p: {"p50": serve[p]["latency_p50_s"], "p99": serve[p]["latency_p99_s"]} for p in ("fp32_bulk", "fp64")},
+        "sedov512_periodic": s512,
         "amr": amr,
         "turbulence": turb,
         "batch": batch,
@@ -618,6 +657,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / accuracy leg")
     ap.add_argument("--acc-steps", type=int, default=100, help="steps before the accuracy comparison")
+    ap.add_argument("--sedov512-steps", type=int, default=5, help="periodic Sedov 512^3 steps (0: skip)")
     ap.add_argument("--amr-steps", type=int, default=10, help="AMR Sedov coarse steps (0: skip)")
     ap.add_argument("--turb-steps", type=int, default=100, help="turbulence 256^3 steps (0: skip)")
     ap.add_argument("--batch-problems", type=int, default=1024, help="batched ensemble size (0: skip)")

@@ -134,6 +134,18 @@ class Mesh:
             self.uold[sl, v, :] = dense[v, cells[..., 2], cells[..., 1], cells[..., 0]]
 
 
+def _demorton3(key, bits=21):
+    """Inverse of :func:`_morton3`: (x, y, z) of interleaved keys."""
+    key = np.asarray(key, np.int64)
+    out = []
+    for d in range(3):
+        v = np.zeros(key.shape, dtype=np.int64)
+        for b in range(bits):
+            v |= ((key >> (3 * b + d)) & 1) << b
+        out.append(v)
+    return out
+
+
 def uniform_mesh(level, nsubgrid=1, boxlen=1.0, bc="outflow", gravity=(0.0, 0.0, 0.0), box_nx=(1, 1, 1)):
     """A single-level mesh (levelmin = levelmax = level) covering its box.
 
@@ -143,6 +155,17 @@ def uniform_mesh(level, nsubgrid=1, boxlen=1.0, bc="outflow", gravity=(0.0, 0.0,
     """
     no = [int(box_nx[d]) << (level - 1) for d in range(3)]
     assert all(n % nsubgrid == 0 for n in no), "octs per edge must be a multiple of nsubgrid"
+    if nsubgrid == 1 and tuple(box_nx) == (1, 1, 1):
+        # a 2^k cube: the Morton keys of its octs are exactly 0 .. N-1
+        key = np.arange(no[0] ** 3, dtype=np.int64)
+        x, y, z = _demorton3(key, bits=level)
+        grid = np.zeros(len(key), dtype=OCT_DTYPE)
+        grid["ckey"][:, 0] = x
+        grid["ckey"][:, 1] = y
+        grid["ckey"][:, 2] = z
+        grid["lev"] = level
+        grid["hkey"] = key
+        return Mesh(grid, level, level, nsubgrid=1, boxlen=boxlen, bc=bc, gravity=gravity, box_nx=box_nx)
     ix, iy, iz = np.meshgrid(np.arange(no[0]), np.arange(no[1]), np.arange(no[2]), indexing="ij")
     ix, iy, iz = ix.ravel(), iy.ravel(), iz.ravel()
     n = nsubgrid
@@ -185,21 +208,33 @@ def sedov3d(mesh, gamma=1.4, rho0=1.0, p0=1e-5, energy=1.0, radius_cells=2.0, ce
     dxf = mesh.dx(lmax)
     c = np.array(centre if centre is not None else
                  [0.5 * mesh.boxlen * mesh.box_nx[d] for d in range(3)])
-    xf = mesh.cell_centres(lmax)
-    rf = np.sqrt(((xf - c) ** 2).sum(-1))
-    n_in = int((rf <= radius_cells * dxf * (1 + 1e-12)).sum())
+    rad = radius_cells * dxf * (1 + 1e-12)
+
+    def near(lev):
+        """Octs of a level whose cells can lie within the radius, and the
+        centre distances of their cells (same arithmetic as cell_centres)."""
+        ck = mesh.grid[mesh.level_slice(lev)]["ckey"].astype(np.int64)
+        dx = mesh.dx(lev)
+        oc = (2 * ck + 1) * dx
+        cand = np.nonzero(np.sqrt(((oc - c) ** 2).sum(-1)) <= rad + 2 * dx)[0]
+        x = ((2 * ck[cand][:, None, :] + CELL_OFF[None, :, :]) + 0.5) * dx
+        return cand, np.sqrt(((x - c) ** 2).sum(-1))
+
+    cand, rf = near(lmax)
+    n_in = int((rf <= rad).sum())
     assert n_in > 0
     p_in = (gamma - 1.0) * energy / (n_in * dxf ** 3)
+    amb = prim_to_cons(np.float64(rho0), 0.0, 0.0, 0.0, np.float64(p0), gamma)
+    blast = prim_to_cons(np.float64(rho0), 0.0, 0.0, 0.0, np.float64(p_in), gamma)
     for lev in range(mesh.levelmin, mesh.levelmax + 1):
         if not mesh.noct[lev]:
             continue
-        x = mesh.cell_centres(lev)
-        r = np.sqrt(((x - c) ** 2).sum(-1))
-        inside = r <= radius_cells * dxf * (1 + 1e-12)
-        rho = np.full(r.shape, rho0)
-        z = np.zeros(r.shape)
-        p = np.where(inside, p_in, p0)
-        set_level_prim(mesh, lev, rho, z, z, z, p, gamma)
+        sl = mesh.level_slice(lev)
+        mesh.uold[sl] = amb[None, :, None]
+        cand, r = near(lev)
+        o, cell = np.nonzero(r <= rad)
+        for v in range(5):
+            mesh.uold[sl.start + cand[o], v, cell] = blast[v]
     return n_in, p_in
 
 
