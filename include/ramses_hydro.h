@@ -143,6 +143,34 @@ int rh_godunov(int head_idx, int num_subgrids, int ngridmax, int ilevel,
                double smallc2, double dt, double dx, double smax_cap,
                int slope, int riemann, const double* constant_gravity);
 
+/* Restriction: the refined cells of level ilevel take the average of their
+ * child octs, head_idx/num_octs being level ilevel+1's octs (1-based), with
+ * internal energy averaged instead of total energy when internal_energy != 0
+ * (interpol_var == 1).  Replaces gpu_upload (gpu/gpu_runner.cuf:1754-1784) and
+ * mtl_upload (metal/metal_runner.f90:814-837), i.e. upload_fine
+ * (hydro/upload.f90:74-271); called after rh_set_uold of level ilevel
+ * (amr/amr_step.f90:479-483).  Asynchronous. */
+int rh_upload(int head_idx, int num_octs, int internal_energy, double gamma,
+              double smallr, double smallc2);
+
+/* Gradient refinement criteria of hydro_refine (hydro/godunov_utils.f90:
+ * 6-223): a criterion is off when its err_grad is negative. */
+typedef struct rh_flag_params {
+    double err_grad_d, err_grad_p, err_grad_u;
+    double floor_d, floor_p, floor_u;
+} rh_flag_params;
+
+/* Refinement flags of the cells of level ilevel by the gradient criteria:
+ * every cell is compared with its six neighbours at the same level (or, where
+ * a neighbour oct does not exist, with that neighbour's parent cell); flag1 is
+ * the host's (1:8, 1:ngridmax) int32 array: flagged cells get 1 (others keep
+ * their value) and *nflag returns how many were newly flagged.  Replaces the
+ * gradient branch of hydro_flag (hydro/hydro_flag.f90:7-159); the reference's
+ * GPU flagging kernel is hydro_flag_kernel (gpu/gpu_hydro.cuf:6690).
+ * Synchronous (the flags are on the host on return). */
+int rh_hydro_flag(int ilevel, const rh_flag_params* f, double gamma, double smallr,
+                  int32_t* flag1, long long* nflag);
+
 /* Extra hydro parameters the reference passes through hydro_params_t but
  * mtl_godunov does not carry (interpolation scheme for coarse-fine ghosts). */
 int rh_set_interpolation(int interpol_var, int interpol_type);

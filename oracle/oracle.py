@@ -13,7 +13,7 @@ import subprocess
 
 import numpy as np
 
-from ramses2_b200._abi import HydroParams, MeshDesc, dptr
+from ramses2_b200._abi import FlagParams, HydroParams, MeshDesc, dptr
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librh_oracle.so")
@@ -41,6 +41,9 @@ def lib():
         L.rh_oracle_interpol_hydro.argtypes = [P(C.c_double), P(C.c_double), C.c_int, C.c_int, C.c_double]
         L.rh_oracle_godunov_fine.argtypes = [P(MeshDesc), P(HydroParams), C.c_int, C.c_double,
                                              P(C.c_double), P(C.c_double), C.c_int]
+        L.rh_oracle_upload_fine.argtypes = [P(MeshDesc), P(HydroParams), C.c_int, P(C.c_double)]
+        L.rh_oracle_hydro_flag.argtypes = [P(MeshDesc), P(HydroParams), P(FlagParams), C.c_int, P(C.c_double),
+                                           P(C.c_int32), P(C.c_longlong)]
         L.rh_oracle_courant_fine.argtypes = [P(MeshDesc), P(HydroParams), C.c_int, P(C.c_double),
                                              P(C.c_double)]
         L.rh_oracle_last_error.restype = C.c_char_p
@@ -115,6 +118,20 @@ class OracleHydro:
     def godunov_fine(self, ilevel, dt):
         _check(lib().rh_oracle_godunov_fine(C.byref(self.mesh.desc()), C.byref(self.params), ilevel,
                                             dt, dptr(self.mesh.uold), dptr(self.unew), self.nthreads))
+
+    def upload_fine(self, ilevel):
+        """Restriction of level ilevel+1 into level ilevel (hydro/upload.f90:74-271)."""
+        _check(lib().rh_oracle_upload_fine(C.byref(self.mesh.desc()), C.byref(self.params), ilevel,
+                                           dptr(self.mesh.uold)))
+
+    def hydro_flag(self, ilevel, flags, flag1):
+        """Gradient branch of hydro_flag (hydro/hydro_flag.f90:7-159) on the
+        (ngridmax, 8) int32 flag1; returns the newly flagged count."""
+        n = C.c_longlong()
+        _check(lib().rh_oracle_hydro_flag(C.byref(self.mesh.desc()), C.byref(self.params), C.byref(flags), ilevel,
+                                          dptr(self.mesh.uold), flag1.ctypes.data_as(C.POINTER(C.c_int32)),
+                                          C.byref(n)))
+        return n.value
 
     def step_uniform(self, dt=None):
         """One coarse step of a single-level run (amr/amr_step.f90:276-455 order)."""

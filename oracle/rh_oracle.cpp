@@ -966,6 +966,178 @@ int rh_oracle_godunov_fine(const rh_mesh_desc* m, const rh_hydro_params* p, int 
   return rc;
 }
 
+// upload_fine, hydro/upload.f90:74-271 (no MHD, no NENER): zero the refined
+// cells of level ilevel, then give each parent cell of a level ilevel+1 oct the
+// average of the oct's eight cells (internal energy averaged instead of total
+// energy when interpol_var == 1).
+int rh_oracle_upload_fine(const rh_mesh_desc* m, const rh_hydro_params* p, int ilevel, double* uold) {
+  if (!m || ilevel < 1 || ilevel >= m->levelmax) { g_err = "bad mesh/level"; return RH_EINVAL; }
+  for (int i = 0; i < m->noct[ilevel]; ++i) {
+    int ig = m->head[ilevel] + i;
+    for (int v = 0; v < 5; ++v)
+      for (int ind = 0; ind < 8; ++ind)
+        if (m->grid[ig - 1].refined[ind]) uold[(size_t)(ig - 1) * 40 + ind + 8 * v] = 0.0;
+  }
+  std::unordered_map<uint64_t, int> dict;
+  for (int i = 0; i < m->noct[ilevel]; ++i) {
+    int ig = m->head[ilevel] + i;
+    const rh_oct& o = m->grid[ig - 1];
+    dict[pack_key(o.lev, o.ckey[0], o.ckey[1], o.ckey[2])] = ig;
+  }
+  for (int i = 0; i < m->noct[ilevel + 1]; ++i) {
+    int io = m->head[ilevel + 1] + i;
+    const rh_oct& o = m->grid[io - 1];
+    // get_parent_cell (amr/nbors_utils.f90:222-249): father key = key / 2
+    int64_t hf[3], ii[3];
+    for (int d = 0; d < 3; ++d) {
+      hf[d] = (int64_t)o.ckey[d] / 2;
+      ii[d] = (int64_t)o.ckey[d] - 2 * hf[d];
+    }
+    int icell = (int)(ii[0] + 2 * ii[1] + 4 * ii[2]);  // 0-based
+    auto it = dict.find(pack_key(ilevel, hf[0], hf[1], hf[2]));
+    if (it == dict.end()) { g_err = "upload: parent oct missing"; return RH_EINVAL; }
+    int igrid = it->second;
+    const double* u = uold + (size_t)(io - 1) * 40;
+    double* up = uold + (size_t)(igrid - 1) * 40;
+    for (int v = 0; v < 5; ++v) {
+      double average = 0.0;
+      for (int ind = 0; ind < 8; ++ind) average = average + u[ind + 8 * v];
+      up[icell + 8 * v] = average / 8.0;
+    }
+    if (p->interpol_var == 1) {
+      double average = 0.0;
+      for (int ind = 0; ind < 8; ++ind) {
+        double ekin = 0.0;
+        for (int d = 1; d <= 3; ++d)
+          ekin = ekin + 0.5 * (u[ind + 8 * d] * u[ind + 8 * d]) / fmax2(u[ind], p->smallr);
+        average = average + u[ind + 32] - ekin;
+      }
+      double ekin = 0.0;
+      for (int d = 1; d <= 3; ++d)
+        ekin = ekin + 0.5 * (up[icell + 8 * d] * up[icell + 8 * d]) / fmax2(up[icell], p->smallr);
+      up[icell + 32] = average / 8.0 + ekin;
+    }
+  }
+  return 0;
+}
+
+// hydro_refine's gradient criteria (hydro/godunov_utils.f90:6-223, no MHD, no
+// NENER, no chemistry): ug/um/ud = left/centre/right conserved states.
+static bool hydro_refine(const double* ug_in, const double* um_in, const double* ud_in, const rh_hydro_params* p,
+                         const rh_flag_params* f) {
+  double ug[5], um[5], ud[5];
+  for (int v = 0; v < 5; ++v) { ug[v] = ug_in[v]; um[v] = um_in[v]; ud[v] = ud_in[v]; }
+  ug[0] = fmax2(ug[0], p->smallr);
+  um[0] = fmax2(um[0], p->smallr);
+  ud[0] = fmax2(ud[0], p->smallr);
+  for (int d = 1; d <= 3; ++d) { ug[d] = ug[d] / ug[0]; um[d] = um[d] / um[0]; ud[d] = ud[d] / ud[0]; }
+  double eking = 0, ekinm = 0, ekind = 0;
+  for (int d = 1; d <= 3; ++d) {
+    eking = eking + 0.5 * ug[0] * (ug[d] * ug[d]);
+    ekinm = ekinm + 0.5 * um[0] * (um[d] * um[d]);
+    ekind = ekind + 0.5 * ud[0] * (ud[d] * ud[d]);
+  }
+  const double gm1 = p->gamma - 1.0;
+  const double pg = gm1 * (ug[4] - eking), pm = gm1 * (um[4] - ekinm), pd = gm1 * (ud[4] - ekind);
+  bool ok = false;
+  if (f->err_grad_d >= 0.) {
+    double e = 2.0 * fmax2(std::fabs((ud[0] - um[0]) / (ud[0] + um[0] + f->floor_d)),
+                           std::fabs((um[0] - ug[0]) / (um[0] + ug[0] + f->floor_d)));
+    ok = ok || e > f->err_grad_d;
+  }
+  if (f->err_grad_p >= 0.) {
+    double e = 2.0 * fmax2(std::fabs((pd - pm) / (pd + pm + f->floor_p)), std::fabs((pm - pg) / (pm + pg + f->floor_p)));
+    ok = ok || e > f->err_grad_p;
+  }
+  if (f->err_grad_u >= 0.) {
+    const double fu2 = f->floor_u * f->floor_u;
+    double cg = std::sqrt(fmax2(p->gamma * pg / ug[0], fu2));
+    double cm = std::sqrt(fmax2(p->gamma * pm / um[0], fu2));
+    double cd = std::sqrt(fmax2(p->gamma * pd / ud[0], fu2));
+    for (int d = 1; d <= 3; ++d) {
+      double vg = ug[d], vm = um[d], vd = ud[d];
+      double e = 2.0 * fmax2(std::fabs((vd - vm) / (cd + cm + std::fabs(vd) + std::fabs(vm) + f->floor_u)),
+                             std::fabs((vm - vg) / (cm + cg + std::fabs(vm) + std::fabs(vg) + f->floor_u)));
+      ok = ok || e > f->err_grad_u;
+    }
+  }
+  return ok;
+}
+
+// hydro_flag's gradient branch (hydro/hydro_flag.f90:7-159): for every cell
+// of the level, the six neighbour cells at the same level, or the parent cell
+// of a missing neighbour; periodic wrap; a neighbour outside a non-periodic
+// box is the boundary ghost, whose density and pressure equal the boundary
+// cell's for zero-gradient and reflexive boundaries (amr/boundaries.f90).
+// Sets flag1[(igrid-1)*8 + ind] = 1 for flagged cells, returns the number of
+// newly flagged cells in *nflag.
+int rh_oracle_hydro_flag(const rh_mesh_desc* m, const rh_hydro_params* p, const rh_flag_params* f, int ilevel,
+                         const double* uold, int* flag1, long long* nflag) {
+  if (!m || ilevel < 1 || ilevel > m->levelmax) { g_err = "bad mesh/level"; return RH_EINVAL; }
+  std::unordered_map<uint64_t, int> dict;
+  for (int l = 1; l <= m->levelmax; ++l)
+    for (int i = 0; i < m->noct[l]; ++i) {
+      int ig = m->head[l] + i;
+      const rh_oct& o = m->grid[ig - 1];
+      dict[pack_key(o.lev, o.ckey[0], o.ckey[1], o.ckey[2])] = ig;
+    }
+  auto find = [&](int lev, int64_t x, int64_t y, int64_t z) -> int {
+    auto it = dict.find(pack_key(lev, x, y, z));
+    return it == dict.end() ? 0 : it->second;
+  };
+  long long newly = 0;
+  for (int i = 0; i < m->noct[ilevel]; ++i) {
+    int ig = m->head[ilevel] + i;
+    const rh_oct& o = m->grid[ig - 1];
+    for (int ind = 0; ind < 8; ++ind) {
+      int64_t cc[3] = {2 * (int64_t)o.ckey[0] + (ind & 1), 2 * (int64_t)o.ckey[1] + ((ind >> 1) & 1),
+                       2 * (int64_t)o.ckey[2] + (ind >> 2)};
+      const double* um_p = uold + (size_t)(ig - 1) * 40 + ind;
+      double um[5];
+      for (int v = 0; v < 5; ++v) um[v] = um_p[8 * v];
+      double nb[6][5];
+      for (int n = 0; n < 6; ++n) {
+        int d = n / 2, sgn = (n & 1) ? 1 : -1;
+        int64_t k[3] = {cc[0], cc[1], cc[2]};
+        k[d] += sgn;
+        int64_t ncell = (int64_t)m->box_nx[d] << ilevel;
+        bool self = false;
+        if (m->periodic[d]) {
+          if (k[d] < 0) k[d] = ncell - 1;
+          if (k[d] >= ncell) k[d] = 0;
+        } else if (k[d] < 0 || k[d] >= ncell) {
+          self = true;
+        }
+        const double* src = nullptr;
+        if (self) {
+          src = um_p;
+        } else {
+          int64_t ok_[3] = {floordiv2(k[0]), floordiv2(k[1]), floordiv2(k[2])};
+          int g2 = find(ilevel, ok_[0], ok_[1], ok_[2]);
+          if (g2 > 0) {
+            int c2 = (int)((k[0] - 2 * ok_[0]) + 2 * (k[1] - 2 * ok_[1]) + 4 * (k[2] - 2 * ok_[2]));
+            src = uold + (size_t)(g2 - 1) * 40 + c2;
+          } else {
+            int64_t fk[3] = {floordiv2(ok_[0]), floordiv2(ok_[1]), floordiv2(ok_[2])};
+            int g3 = find(ilevel - 1, fk[0], fk[1], fk[2]);
+            if (g3 == 0) { g_err = "hydro_flag: neither a neighbour nor its parent cell exists"; return RH_EINVAL; }
+            int c3 = (int)((ok_[0] - 2 * fk[0]) + 2 * (ok_[1] - 2 * fk[1]) + 4 * (ok_[2] - 2 * fk[2]));
+            src = uold + (size_t)(g3 - 1) * 40 + c3;
+          }
+        }
+        for (int v = 0; v < 5; ++v) nb[n][v] = src[8 * v];
+      }
+      bool ok = false;
+      for (int d = 0; d < 3; ++d) ok = hydro_refine(nb[2 * d], um, nb[2 * d + 1], p, f) || ok;
+      int& fl = flag1[(size_t)(ig - 1) * 8 + ind];
+      if (fl == 0 && ok) ++newly;
+      if (ok) fl = 1;
+    }
+  }
+  if (nflag) *nflag = newly;
+  return 0;
+}
+
 int rh_oracle_courant_fine(const rh_mesh_desc* m, const rh_hydro_params* p, int ilevel,
                            const double* uold, double* out) {
   if (!m || ilevel < 1 || ilevel > m->levelmax) { g_err = "bad mesh/level"; return RH_EINVAL; }

@@ -63,6 +63,16 @@ int rh_oracle_courant_fine(const rh_mesh_desc* m, const rh_hydro_params* p,
 
 const char* rh_oracle_last_error(void);
 
+/* upload_fine: restriction of level ilevel+1 into the refined cells of level
+ * ilevel, in place on uold (hydro/upload.f90:74-271). */
+int rh_oracle_upload_fine(const rh_mesh_desc* m, const rh_hydro_params* p, int ilevel, double* uold);
+
+/* hydro_flag's gradient branch (hydro/hydro_flag.f90:7-159 with
+ * hydro_refine, hydro/godunov_utils.f90:6-223) for the cells of a level;
+ * flag1 is (1:8, 1:ngridmax) int32. */
+int rh_oracle_hydro_flag(const rh_mesh_desc* m, const rh_hydro_params* p, const rh_flag_params* f, int ilevel,
+                         const double* uold, int* flag1, long long* nflag);
+
 #ifdef __cplusplus
 }
 #endif

@@ -117,3 +117,14 @@ class BatchIC(C.Structure):
         ("centre", C.c_double * 3),
         ("host_uold", C.c_void_p),
     ]
+
+
+class FlagParams(C.Structure):
+    """rh_flag_params: hydro_refine's gradient criteria (negative = off)."""
+
+    _fields_ = [("err_grad_d", C.c_double), ("err_grad_p", C.c_double), ("err_grad_u", C.c_double),
+                ("floor_d", C.c_double), ("floor_p", C.c_double), ("floor_u", C.c_double)]
+
+    @classmethod
+    def make(cls, err_grad_d=-1.0, err_grad_p=-1.0, err_grad_u=-1.0, floor_d=1e-10, floor_p=1e-10, floor_u=1e-10):
+        return cls(err_grad_d, err_grad_p, err_grad_u, floor_d, floor_p, floor_u)

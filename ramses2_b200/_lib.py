@@ -6,7 +6,7 @@ entry point of this package raises.
 import ctypes as C
 import os
 
-from ._abi import STATUS, BatchIC, BatchProblem, HydroParams, MeshDesc
+from ._abi import STATUS, BatchIC, BatchProblem, FlagParams, HydroParams, MeshDesc
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librh_b200.so")
@@ -32,6 +32,8 @@ SIGNATURES = {
     "rh_cmpdt": (_i, [_i, _i, _d, _d, _d, _d, _d, _P(_d), _P(_d), _P(_d), _P(_d), _P(_d), _P(_d)]),
     "rh_godunov": (_i, [_i, _i, _i, _i, _i, _i, _d, _d, _d, _d, _d, _d, _i, _i, _P(_d)]),
     "rh_set_interpolation": (_i, [_i, _i]),
+    "rh_upload": (_i, [_i, _i, _i, _d, _d, _d]),
+    "rh_hydro_flag": (_i, [_i, _P(FlagParams), _d, _d, _P(C.c_int32), _P(C.c_longlong)]),
     # extensions (include/ramses_hydro_ext.h)
     "rh_set_tile": (_i, [_i, _i, _i, _i]),
     "rh_get_tile": (_i, [_P(_i), _P(_i), _P(_i), _P(_i)]),

@@ -237,8 +237,12 @@ static void free_state() {
   cudaFree(c.d_scratch);
   cudaFree(c.d_refmask);
   cudaFree(c.d_gfather);
+  cudaFree(c.d_father);
+  for (auto* f : c.d_face) cudaFree(f);
+  c.d_face.clear();
   c.d_refmask = nullptr;
   c.d_gfather = nullptr;
+  c.d_father = nullptr;
   c.d_cfl = nullptr;
   c.d_scratch = nullptr;
   c.scratch_elems = 0;

@@ -78,6 +78,8 @@ struct Context {
   long long nstate = 0;            // ngridmax + interpolated ghost octs of all levels
   uint8_t* d_refmask = nullptr;    // [nstate] refined-cell bits (ghosts: 0)
   int2* d_gfather = nullptr;       // [nstate - ngridmax] father of each ghost
+  int2* d_father = nullptr;        // [ngridmax] father (oct, cell) of each oct, built by the first rh_upload
+  std::vector<int2*> d_face;       // per level: [noct][6] cells across each face (rh_hydro_flag)
   int nlevels_used = 0;
   int* d_err = nullptr;
   double* d_cfl = nullptr;        // [levelmax+1][5] reduced CFL values

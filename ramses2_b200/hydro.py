@@ -66,6 +66,25 @@ class GodunovGPU:
                                 P.smallc ** 2, dt, dx, smax_cap, P.slope_type, P.riemann, dptr(self._grav)),
               "rh_godunov")
 
+    def upload_fine(self, ilevel):
+        """Restriction of level ilevel+1 into the refined cells of level ilevel."""
+        m = self.mesh
+        P = self.params
+        if ilevel >= m.levelmax or not m.noct[ilevel + 1]:
+            return
+        check(self.L.rh_upload(int(m.head[ilevel + 1]), int(m.noct[ilevel + 1]), int(P.interpol_var == 1),
+                               P.gamma, P.smallr, P.smallc ** 2), "rh_upload")
+
+    def hydro_flag(self, ilevel, flags, flag1):
+        """Gradient refinement flags of level ilevel (hydro_flag): flag1 is the
+        (ngridmax, 8) int32 array of the host; returns the newly flagged count."""
+        assert flag1.dtype == np.int32 and flag1.flags.c_contiguous and flag1.size == 8 * self.mesh.ngridmax
+        n = C.c_longlong()
+        P = self.params
+        check(self.L.rh_hydro_flag(int(ilevel), C.byref(flags), P.gamma, P.smallr,
+                                   flag1.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(n)), "rh_hydro_flag")
+        return n.value
+
     # ---- conveniences -----------------------------------------------------------
     def step_uniform(self, dt=None):
         """One coarse step of a single-level run in the reference's order."""
@@ -133,5 +152,7 @@ def amr_coarse_step(solver, mesh, dt=None):
     for l in reversed(lev):
         solver.godunov_fine(l, dt)
         solver.set_uold(l)
+        if l < lev[-1]:
+            solver.upload_fine(l)
     return dt
 

@@ -258,3 +258,70 @@ def test_amr_step_fp32_bulk():
         gpu.close()
     assert err[0] <= TOL_FP32_RHO, err
     assert np.all(err <= 1e-4), err
+
+
+@pytest.mark.parametrize("ivar", [0, 1])
+def test_upload_fine_matches_oracle_bitwise(ivar):
+    """Restriction (hydro/upload.f90:74-271) of every level into its parent
+    cells, FP64: bitwise equal to the oracle; FP32-bulk: within FP32 rounding."""
+    m, P = amr_case("outflow", 1, ivar)
+    u0 = m.uold.copy()
+    o = oracle.OracleHydro(m, P, nthreads=1)
+    lev = [l for l in range(m.levelmin, m.levelmax + 1) if m.noct[l]]
+    for l in reversed(lev[:-1]):
+        o.upload_fine(l)
+    ref = m.uold.copy()
+    assert not np.array_equal(ref, u0)
+    for prec, tol in (("fp64", 0.0), ("fp32_bulk", 1e-6)):
+        m.uold[:] = u0
+        gpu = GodunovGPU(m, P, precision=prec)
+        try:
+            for l in reversed(lev[:-1]):
+                gpu.upload_fine(l)
+            out = gpu.fetch_uold()
+        finally:
+            gpu.close()
+        if tol == 0.0:
+            assert np.array_equal(out, ref)
+        else:
+            assert np.all(rel_l1(out, ref) <= tol), rel_l1(out, ref)
+
+
+@pytest.mark.parametrize("case", ["amr", "outflow", "periodic", "reflexive"])
+def test_hydro_flag_matches_oracle(case):
+    """Gradient refinement flags (hydro_flag + hydro_refine): FP64 flags equal
+    the oracle's cell for cell, including neighbours taken from parent cells
+    across coarse-fine faces and from boundary ghosts; cells already flagged
+    are not counted again."""
+    from ramses2_b200._abi import FlagParams
+    from ramses2_b200.mesh import sedov_amr_mesh
+
+    if case == "amr":
+        m, g = sedov_amr_mesh(4, 6, radius=0.25)
+        F = FlagParams.make(err_grad_d=0.1, err_grad_p=0.1)
+    else:
+        m = uniform_mesh(5, nsubgrid=1, bc=case)
+        g = blast_state(m, 21, 1.4)
+        F = FlagParams.make(err_grad_d=0.2, err_grad_p=0.3, err_grad_u=0.5)
+    P = HydroParams.make(gamma=g)
+    lev = [l for l in range(m.levelmin, m.levelmax + 1) if m.noct[l]]
+    o = oracle.OracleHydro(m, P)
+    pre = np.zeros((m.ngridmax, 8), np.int32)
+    pre[::7, 3] = 1
+    ref, nref = pre.copy(), []
+    for l in lev:
+        nref.append(o.hydro_flag(l, F, ref))
+    assert sum(nref) > 0
+    for prec in ("fp64", "fp32_bulk"):
+        gpu = GodunovGPU(m, P, precision=prec)
+        try:
+            out, nout = pre.copy(), []
+            for l in lev:
+                nout.append(gpu.hydro_flag(l, F, out))
+        finally:
+            gpu.close()
+        if prec == "fp64":
+            assert np.array_equal(out, ref)
+            assert nout == nref
+        else:
+            assert np.mean(out != ref) <= 5e-3

@@ -289,3 +289,46 @@ def test_interpol_hydro_conservative(itype, ivar):
         assert np.allclose(u2[4].mean(), u1[4, 0], rtol=1e-13)
     if itype == 0 and ivar == 0:
         assert np.array_equal(u2, np.repeat(u1[:, :1], 8, axis=1))
+
+
+def test_amr_step_conserves_mass_and_energy_periodic():
+    """Coarse-fine levels of the oracle: three coarse steps (courant_fine,
+    godunov_fine with the coarse-cell flux corrections, set_uold and the
+    restriction upload_fine, amr/amr_step.f90 order with nsubcycle=1) of a
+    three-level periodic mesh keep the leaf-cell totals of mass and energy at
+    round-off."""
+    import math
+
+    from ramses2_b200.hydro import amr_coarse_step
+    from ramses2_b200.mesh import amr_mesh, fill_amr_prim
+
+    m = amr_mesh(3, 5, lambda x, l: np.sqrt(((x - 0.52) ** 2).sum(-1)) < 0.2, bc="periodic")
+
+    def prim(x, l):
+        r = np.sqrt(((x - 0.5) ** 2).sum(-1))
+        z = np.zeros_like(r)
+        return 1 + 0.5 * np.exp(-r ** 2 / 0.01), 0.3 + z, -0.2 + z, 0.1 + z, 1 + 4 * np.exp(-r ** 2 / 0.004)
+
+    fill_amr_prim(m, prim, 1.4)
+    P = HydroParams.make(gamma=1.4, courant_factor=0.5, slope_type=2, riemann="hllc", interpol_type=1)
+    o = oracle.OracleHydro(m, P, nthreads=4)
+    lev = [l for l in range(m.levelmin, m.levelmax + 1) if m.noct[l]]
+    for l in reversed(lev[:-1]):
+        o.upload_fine(l)
+
+    def totals():
+        out = []
+        for v in (0, 4):
+            parts = []
+            for l in lev:
+                sl = m.level_slice(l)
+                parts.append((m.uold[sl, v, :] * m.leaf_mask(l)).ravel() * m.dx(l) ** 3)
+            out.append(math.fsum(np.concatenate(parts)))
+        return out
+
+    t0 = totals()
+    for _ in range(3):
+        amr_coarse_step(o, m)
+    t1 = totals()
+    assert t1[0] == pytest.approx(t0[0], rel=1e-13)
+    assert t1[1] == pytest.approx(t0[1], rel=1e-13)
