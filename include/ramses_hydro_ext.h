@@ -24,6 +24,10 @@ int rh_get_tile(int* txo, int* tyo, int* minb, int* lz);
 int rh_list_tiles(int precision, int* txo, int* tyo, int* minb, int max);
 /* Pencil count and oct-table size of a level's current tables. */
 int rh_level_info(int ilevel, int* npencil, long long* table_entries);
+/* Copy a level's pencil headers (npencil x int4: ox0, oy0, oz0, layers),
+ * table offsets (npencil) and oct table (entries: 0-based oct index per
+ * (pencil, layer row, oct column), boundary-resolved) to the host. */
+int rh_level_table(int ilevel, int* phdr, long long* poff, int* tab, long long max_entries);
 /* Device pointers of the current uold / unew buffers (FP64: *_d is
  * [oct][5][8]; FP32-bulk: *_f is [oct][4][8] float, *_d is [oct][8] energy). */
 int rh_state_ptrs(void** uold_d, void** uold_f, void** unew_d, void** unew_f);

@@ -180,6 +180,7 @@ int build_amr_tables(int l, const TileCfg& cfg, long long gbase) {
   }
   T.nghost = (int)T.gfather.size();
   T.npencil = (int)T.phdr.size();
+  T.ntab = (long long)T.ptab.size();
   T.complete = false;
   return RH_OK;
 }

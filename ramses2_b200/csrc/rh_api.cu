@@ -249,86 +249,25 @@ static void free_state() {
   c.have_mesh = false;
 }
 
-// Oct index (0-based) at level-l oct coordinates, after periodic wrap /
-// non-periodic clamp (zero-gradient and reflexive ghosts both take their
-// cells from the adjacent interior oct: amr/boundaries.f90:150-216).
-static inline long long wrap_clamp(long long v, long long n, int periodic) {
-  if (periodic) {
-    v %= n;
-    if (v < 0) v += n;
-    return v;
-  }
-  return v < 0 ? 0 : (v >= n ? n - 1 : v);
-}
-
-// Build the pencil tables of a complete (uniform) level.
+// Build the pencil tables of a complete (uniform) level (on the device:
+// rh_tables.cu) and upload the pencil headers.
 static int build_level_tables(int l, const TileCfg& cfg) {
   Context& c = ctx();
   LevelTables& T = c.levels[l];
   free_tables(T);
   T.cfg = cfg;
-  const long long nx = (long long)c.box_nx[0] << (l - 1), ny = (long long)c.box_nx[1] << (l - 1),
-                  nz = (long long)c.box_nx[2] << (l - 1);
-  T.nxo = (int)nx;
-  T.nyo = (int)ny;
-  T.nzo = (int)nz;
-  if ((long long)c.noct[l] != nx * ny * nz) {
-    set_error("level %d has %d octs, its box holds %lld: coarse-fine levels need the AMR table builder", l,
-              c.noct[l], nx * ny * nz);
-    return RH_EINVAL;
-  }
-  std::vector<int> idx((size_t)(nx * ny * nz), -1);
-  for (int i = 0; i < c.noct[l]; ++i) {
-    const rh_oct& o = c.grid[(size_t)c.head[l] - 1 + i];
-    long long x = o.ckey[0], y = o.ckey[1], z = o.ckey[2];
-    if (o.lev != l || x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) {
-      set_error("oct %d of level %d has key (%lld,%lld,%lld) outside its box", c.head[l] + i, l, x, y, z);
-      return RH_EINVAL;
-    }
-    size_t k = (size_t)((z * ny + y) * nx + x);
-    if (idx[k] >= 0) {
-      set_error("duplicate oct key at level %d", l);
-      return RH_EINVAL;
-    }
-    idx[k] = c.head[l] - 1 + i;
-  }
-  const int OW = cfg.txo + 2, OH = cfg.tyo + 2, NS = OW * OH;
-  const long long tx = (nx + cfg.txo - 1) / cfg.txo, ty = (ny + cfg.tyo - 1) / cfg.tyo,
-                  tz = (nz + cfg.lz - 1) / cfg.lz;
-  T.phdr.clear();
-  T.poff.clear();
-  T.ptab.clear();
-  for (long long bz = 0; bz < tz; ++bz)
-    for (long long by = 0; by < ty; ++by)
-      for (long long bx = 0; bx < tx; ++bx) {
-        const int ox0 = (int)(bx * cfg.txo), oy0 = (int)(by * cfg.tyo), oz0 = (int)(bz * cfg.lz);
-        const int L = (int)std::min<long long>(cfg.lz, nz - oz0);
-        T.phdr.push_back(make_int4(ox0, oy0, oz0, L));
-        T.poff.push_back((long long)T.ptab.size());
-        for (int r = 0; r < L + 2; ++r) {
-          const long long z = wrap_clamp(oz0 - 1 + r, nz, c.periodic[2]);
-          for (int j = 0; j < OH; ++j) {
-            const long long y = wrap_clamp(oy0 - 1 + j, ny, c.periodic[1]);
-            for (int i = 0; i < OW; ++i) {
-              const long long x = wrap_clamp(ox0 - 1 + i, nx, c.periodic[0]);
-              T.ptab.push_back(idx[(size_t)((z * ny + y) * nx + x)]);
-            }
-          }
-        }
-      }
+  int rc = build_complete_tables_device(l, cfg, T);
+  if (rc) return rc;
   T.npencil = (int)T.phdr.size();
   RH_CUDA(cudaMalloc(&T.d_phdr, sizeof(int4) * T.phdr.size()));
   RH_CUDA(cudaMalloc(&T.d_poff, sizeof(long long) * T.poff.size()));
-  RH_CUDA(cudaMalloc(&T.d_ptab, sizeof(int) * T.ptab.size()));
   RH_CUDA(cudaMalloc(&T.d_cfl_partial, sizeof(double) * 5 * T.npencil));
   RH_CUDA(cudaMemcpyAsync(T.d_phdr, T.phdr.data(), sizeof(int4) * T.phdr.size(), cudaMemcpyHostToDevice, c.stream));
   RH_CUDA(cudaMemcpyAsync(T.d_poff, T.poff.data(), sizeof(long long) * T.poff.size(), cudaMemcpyHostToDevice,
                           c.stream));
-  RH_CUDA(cudaMemcpyAsync(T.d_ptab, T.ptab.data(), sizeof(int) * T.ptab.size(), cudaMemcpyHostToDevice, c.stream));
   RH_CUDA(cudaStreamSynchronize(c.stream));
   T.built = true;
   T.complete = true;
-  (void)NS;
   return RH_OK;
 }
 
@@ -999,13 +938,35 @@ int rh_list_tiles(int precision, int* txo, int* tyo, int* minb, int max) {
   return list_tiles(precision, 0, txo, tyo, minb, max);
 }
 
+int rh_level_table(int ilevel, int* phdr, long long* poff, int* tab, long long max_entries) {
+  int rc = check_ready();
+  if (rc) return rc;
+  Context& c = ctx();
+  if (ilevel < 0 || ilevel > c.levelmax || !c.levels[ilevel].built) {
+    set_error("rh_level_table: level %d has no tables", ilevel);
+    return RH_EINVAL;
+  }
+  const LevelTables& T = c.levels[ilevel];
+  if (max_entries < T.ntab) {
+    set_error("rh_level_table: %lld entries do not fit in %lld", T.ntab, max_entries);
+    return RH_EINVAL;
+  }
+  if (phdr) std::memcpy(phdr, T.phdr.data(), sizeof(int4) * T.phdr.size());
+  if (poff) std::memcpy(poff, T.poff.data(), sizeof(long long) * T.poff.size());
+  if (tab) {
+    RH_CUDA(cudaMemcpyAsync(tab, T.d_ptab, sizeof(int) * T.ntab, cudaMemcpyDeviceToHost, c.stream));
+    RH_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  return RH_OK;
+}
+
 int rh_level_info(int ilevel, int* npencil, long long* table_entries) {
   int rc = check_ready();
   if (rc) return rc;
   Context& c = ctx();
   if (ilevel < 0 || ilevel > c.levelmax) return RH_EINVAL;
   if (npencil) *npencil = c.levels[ilevel].npencil;
-  if (table_entries) *table_entries = (long long)c.levels[ilevel].ptab.size();
+  if (table_entries) *table_entries = c.levels[ilevel].ntab;
   return RH_OK;
 }
 

@@ -44,7 +44,8 @@ struct LevelTables {
   int npencil = 0;
   std::vector<int4> phdr;
   std::vector<long long> poff;
-  std::vector<int> ptab;
+  std::vector<int> ptab;             // host copy (coarse-fine levels only)
+  long long ntab = 0;                // table entries on the device
   int4* d_phdr = nullptr;
   long long* d_poff = nullptr;
   int* d_ptab = nullptr;
@@ -102,5 +103,7 @@ Context& ctx();
 int build_amr_tables(int l, const TileCfg& cfg, long long gbase);
 int upload_amr_tables(int l);
 int prolong_ghosts(int l, double smallr);
+// complete levels (rh_tables.cu)
+int build_complete_tables_device(int l, const TileCfg& cfg, LevelTables& T);
 
 }  // namespace rh

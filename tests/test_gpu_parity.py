@@ -325,3 +325,64 @@ def test_hydro_flag_matches_oracle(case):
             assert nout == nref
         else:
             assert np.mean(out != ref) <= 5e-3
+
+
+def _tables_numpy(m, lev, txo, tyo, lz):
+    """Pencil tables of a complete level, restated in numpy: pencils ordered
+    (bz, by, bx); rows z = oz0-1 .. oz0+L; oct columns (y, x) of the tile
+    plus one-oct halo; coordinates wrapped (periodic) or clamped."""
+    n = [m.box_nx[d] << (lev - 1) for d in range(3)]
+    idx = np.full(n[::-1], -1, dtype=np.int64)  # [z, y, x]
+    g = m.grid[m.level_slice(lev)]
+    ck = g["ckey"].astype(np.int64)
+    idx[ck[:, 2], ck[:, 1], ck[:, 0]] = np.arange(len(g)) + m.head[lev] - 1
+
+    def wc(v, nn, per):
+        return v % nn if per else min(max(v, 0), nn - 1)
+
+    hdr, tab = [], []
+    for bz in range(-(-n[2] // lz)):
+        for by in range(-(-n[1] // tyo)):
+            for bx in range(-(-n[0] // txo)):
+                L = min(lz, n[2] - bz * lz)
+                hdr.append((bx * txo, by * tyo, bz * lz, L))
+                for r in range(L + 2):
+                    z = wc(bz * lz - 1 + r, n[2], m.periodic[2])
+                    for j in range(tyo + 2):
+                        y = wc(by * tyo - 1 + j, n[1], m.periodic[1])
+                        for i in range(txo + 2):
+                            tab.append(idx[z, y, wc(bx * txo - 1 + i, n[0], m.periodic[0])])
+    return np.array(hdr), np.array(tab)
+
+
+@pytest.mark.parametrize("bc,tile,box", [("outflow", (7, 7, 3), (1, 1, 1)), ("periodic", (8, 4, 5), (2, 1, 1)),
+                                         (["periodic", "periodic", "outflow", "outflow", "reflexive", "reflexive"],
+                                          (8, 8, 16), (1, 2, 1))])
+def test_device_built_tables_match_restatement(bc, tile, box):
+    """The device-side table builder of complete levels gives exactly the
+    oct tables of the restated construction (wrap / clamp, pencil order)."""
+    import ctypes as C
+
+    from ramses2_b200._lib import lib
+
+    m = uniform_mesh(4, nsubgrid=1, bc=bc, box_nx=box)
+    sedov3d(m)
+    P = HydroParams.make(gamma=1.4)
+    gpu = GodunovGPU(m, P, tile=tile)
+    try:
+        gpu.step_uniform()  # builds the tables for the tile
+        L = lib()
+        npen, ntab = C.c_int(), C.c_longlong()
+        assert L.rh_level_info(4, C.byref(npen), C.byref(ntab)) == 0
+        hdr = np.zeros((npen.value, 4), np.int32)
+        poff = np.zeros(npen.value, np.int64)
+        tab = np.zeros(ntab.value, np.int32)
+        assert L.rh_level_table(4, hdr.ctypes.data_as(C.POINTER(C.c_int)),
+                                poff.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                tab.ctypes.data_as(C.POINTER(C.c_int)), ntab.value) == 0
+    finally:
+        gpu.close()
+    want_hdr, want_tab = _tables_numpy(m, 4, tile[0], tile[1], tile[2])
+    assert np.array_equal(hdr, want_hdr)
+    assert np.array_equal(tab, want_tab)
+    assert poff[0] == 0 and np.all(np.diff(poff) == (hdr[:-1, 3] + 2) * (tile[0] + 2) * (tile[1] + 2))
