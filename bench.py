@@ -587,7 +587,7 @@ def run_ours(args):
                 "h2d_bytes_per_step": results["e2e_bytes"], "d2h_bytes_per_step": results["e2e_bytes"]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": profile_traffic(prec), "peak_kind": peak_kind,
-                     "kernel": "godunov_pencil_kernel<float>", "kernel_ms": kms,
+                     "kernel": "godunov_pencil2_kernel (FP32-bulk)", "kernel_ms": kms,
                      "bytes_per_cell_update": B_ALG[prec]},
         "cpu_baseline": cpu,
         "accuracy": acc,
