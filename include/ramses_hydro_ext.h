@@ -70,6 +70,12 @@ int rh_cmpdt_noalloc(const double* d_uold, int num_octs, const unsigned char* d_
                      double gamma, double smallr, double smallc, double courant_factor,
                      const double* constant_gravity, double* d_out, void* stream);
 
+/* Runs the pencil kernels' bounded mbarrier wait on a barrier nothing arrives
+ * on (bound polls, at most 2^20): returns RH_ETIMEDOUT through the same error
+ * word rh_sync reads, with the context still usable.  For tests of the
+ * failure path; faults, traps and hangs are never used. */
+int rh_selftest_wait(long long bound);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,6 +44,7 @@ SIGNATURES = {
     "rh_bench_godunov": (_i, [_i, _i, _d, _d, _d, _d, _d, _d, _i, _i, _P(C.c_float)]),
     "rh_timer_start": (_i, []),
     "rh_timer_stop": (_i, [_P(C.c_float)]),
+    "rh_selftest_wait": (_i, [C.c_longlong]),
     # batch (include/ramses_hydro_batch.h)
     "rh_batch_init": (_i, [_i, _i, _i, C.c_longlong]),
     "rh_batch_free": (_i, []),

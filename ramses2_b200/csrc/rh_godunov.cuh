@@ -270,6 +270,25 @@ struct SlotCflSink {
   __device__ __forceinline__ double* out(const LevelArgs&) const { return *p; }
 };
 
+// Wait for an mbarrier phase, polling at most `bound` times.  A CTA whose
+// thread gives up (or sees that another one did) stops waiting, raises the
+// CTA's abort flag and sets bit 0 of the device error word, which the host
+// reads as RH_ETIMEDOUT; the kernel then runs to its end instead of hanging.
+__device__ __forceinline__ bool bounded_mbar_wait(uint64_t* bar, uint32_t par, int* s_abort, int* err,
+                                                  long long bound) {
+  long long it = 0;
+  while (!mbar_try_wait(bar, par)) {
+    if (*s_abort || ++it > bound) {
+      if (!*s_abort) {
+        *s_abort = 1;
+        atomicOr(err, 1);
+      }
+      return false;
+    }
+  }
+  return true;
+}
+
 // Bulk-async staging of the oct layers of a pencil.
 template <typename T, class G, bool DENSE = false> struct Stager {
   double* stageD;
@@ -316,16 +335,7 @@ template <typename T, class G, bool DENSE = false> struct Stager {
   __device__ __forceinline__ void wait(int row) {
     const int st = (rb() + row) % G::NSTAGE;
     const uint32_t par = ((rb() + row) / G::NSTAGE) & 1;
-    long long it = 0;
-    while (!mbar_try_wait(&bar[st], par)) {
-      if (*s_abort || ++it > kWaitBound) {
-        if (!*s_abort) {
-          *s_abort = 1;
-          atomicOr(err, 1);
-        }
-        break;
-      }
-    }
+    bounded_mbar_wait(&bar[st], par, s_abort, err, kWaitBound);
   }
   __device__ __forceinline__ const double* slot_d(int row, int slot) const {
     return stageD + ((size_t)((rb() + row) % G::NSTAGE) * G::NSLOT + slot) * Store<T>::kSlotD;

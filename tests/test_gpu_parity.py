@@ -165,6 +165,24 @@ def test_config0_sedov64_per_step_over_100_steps():
         gpu.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32_bulk"])
+def test_constant_gravity_one_step(precision):
+    """Constant gravity: the half-step velocity predictor of ctoprim
+    (umuscl.f90:1739-1901) and the gravity term of cmpdt
+    (godunov_utils.f90:228-333) against the oracle."""
+    m = uniform_mesh(5, nsubgrid=1, bc="outflow", gravity=(0.3, -0.2, 0.5))
+    g = blast_state(m, 5, 1.4)
+    P = HydroParams.make(gamma=g, courant_factor=0.8, slope_type=2, riemann="hllc")
+    ref, out, (dto, co), (dtg, cg) = run_one_step(m, P, precision=precision)
+    err = rel_l1(out, ref)
+    if precision == "fp64":
+        assert dtg == pytest.approx(dto, rel=1e-13)
+        assert np.all(err <= TOL_FP64), err
+    else:
+        assert dtg == pytest.approx(dto, rel=1e-6)
+        assert err[0] <= TOL_FP32_RHO, err
+
+
 def test_turbulence_one_step_fp64():
     m = uniform_mesh(5, nsubgrid=1, bc="periodic")
     turbulence3d(m, gamma=1.001, mach=5.0)
