@@ -36,6 +36,7 @@ SIGNATURES = {
     "rh_hydro_flag": (_i, [_i, _P(FlagParams), _d, _d, _P(C.c_int32), _P(C.c_longlong)]),
     # extensions (include/ramses_hydro_ext.h)
     "rh_set_tile": (_i, [_i, _i, _i, _i]),
+    "rh_set_amr_tile": (_i, [_i, _i, _i, _i]),
     "rh_get_tile": (_i, [_P(_i), _P(_i), _P(_i), _P(_i)]),
     "rh_list_tiles": (_i, [_i, _P(_i), _P(_i), _P(_i), _i]),
     "rh_level_info": (_i, [_i, _P(_i), _P(C.c_longlong)]),

@@ -432,6 +432,22 @@ int rh_set_tile(int txo, int tyo, int minb, int lz) {
   return RH_OK;
 }
 
+int rh_set_amr_tile(int txo, int tyo, int minb, int lz) {
+  int rc = check_ready(false);
+  if (rc) return rc;
+  Context& c = ctx();
+  if (!find_launcher(c.precision, txo, tyo, minb, 2, 3, 1) || lz < 1) {
+    set_error("coarse-fine tile %dx%d (minb=%d, lz=%d) is not compiled for this precision", txo, tyo, minb, lz);
+    return RH_EINVAL;
+  }
+  if (c.have_mesh && c.nlevels_used > 1) {
+    set_error("rh_set_amr_tile: call before rh_set_mesh (the ghost octs of a mesh follow its tiles)");
+    return RH_ESTATE;
+  }
+  c.amr_cfg = TileCfg{txo, tyo, minb, lz};
+  return RH_OK;
+}
+
 int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotondim) {
   int rc = check_ready(false);
   if (rc) return rc;

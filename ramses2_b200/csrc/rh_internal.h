@@ -54,7 +54,7 @@ struct LevelTables {
 
 struct Context {
   bool inited = false;
-  TileCfg amr_cfg{4, 4, 2, 8};  // tiles of coarse-fine levels
+  TileCfg amr_cfg{8, 4, 2, 8};  // tiles of multi-level meshes (coarse-fine kernels)
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
