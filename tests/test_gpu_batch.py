@@ -276,3 +276,33 @@ def test_batch_pool_admission_and_reuse():
     finally:
         b.close()
 
+
+
+@pytest.mark.parametrize("n,lev,box", [((2, 2, 2), 1, (1, 1, 1)), ((2, 16, 2), 1, (1, 8, 1)),
+                                       ((30, 6, 10), 1, (15, 3, 5)), ((4, 4, 64), 1, (2, 2, 32))])
+def test_batch_edge_shapes_match_oracle(n, lev, box):
+    """Degenerate and ragged boxes (one oct, one-oct-thin, sizes that no tile
+    divides, a pencil deeper than the tile): FP64 batch vs oracle, 2 steps."""
+    rng = np.random.default_rng(sum(n))
+    g = 1.4
+    P = HydroParams.make(gamma=g, courant_factor=0.8, slope_type=2, riemann="hllc")
+    dx = 1.0 / 2 ** lev
+    z, y, x = np.indices((n[2], n[1], n[0]))
+    rho = 1.0 + 0.5 * rng.random((n[2], n[1], n[0]))
+    u = 0.3 * rng.standard_normal((n[2], n[1], n[0]))
+    v = 0.3 * rng.standard_normal((n[2], n[1], n[0]))
+    w = 0.3 * rng.standard_normal((n[2], n[1], n[0]))
+    p = 1.0 + rng.random((n[2], n[1], n[0]))
+    dense = prim_to_cons(rho, u, v, w, p, g)
+    ref, t_ref = oracle_run(dense, lev, box, "outflow", P, 2)
+    b = Batch("fp64", pool_octs=4096)
+    try:
+        pid = b.add(problem(n, dx=dx, bc="outflow", gamma=g, courant_factor=0.8, max_steps=2),
+                    ic_host(dense_to_octs(dense)))
+        b.step(2)
+        out = b.fetch_dense(pid)
+        assert b.status(pid)["t"] == pytest.approx(t_ref, rel=1e-13)
+    finally:
+        b.close()
+    err = rel_l1(out, ref)
+    assert np.all(err <= TOL_FP64), err
