@@ -70,6 +70,8 @@ struct Batch {
   int nslot = 0;
   long long nwork = 0;
   bool dirty = true;             // work list / graph must be rebuilt
+  const void* occ_reg = nullptr; // kernel whose occupancy occ_per_sm holds
+  int occ_per_sm = 0;
   cudaGraphExec_t graph = nullptr;
   int graph_parity = 0;
   int nblocks = 0;
@@ -315,20 +317,21 @@ int rebuild() {
   }
   b.nslot = (int)ids.size();
   b.nwork = woff.back();
-  RH_CUDA(cudaMemcpy(b.d_prob, probs.data(), sizeof(BatchProb) * b.cap, cudaMemcpyHostToDevice));
-  cudaFree(b.d_order);
-  cudaFree(b.d_woff);
-  b.d_order = nullptr;
-  b.d_woff = nullptr;
-  RH_CUDA(cudaMalloc(&b.d_order, sizeof(int) * std::max<size_t>(1, ids.size())));
-  RH_CUDA(cudaMalloc(&b.d_woff, sizeof(long long) * woff.size()));
-  if (!ids.empty()) RH_CUDA(cudaMemcpy(b.d_order, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
-  RH_CUDA(cudaMemcpy(b.d_woff, woff.data(), sizeof(long long) * woff.size(), cudaMemcpyHostToDevice));
+  RH_CUDA(cudaMemcpyAsync(b.d_prob, probs.data(), sizeof(BatchProb) * b.cap, cudaMemcpyHostToDevice, c.stream));
+  if (!ids.empty())
+    RH_CUDA(cudaMemcpyAsync(b.d_order, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice, c.stream));
+  RH_CUDA(cudaMemcpyAsync(b.d_woff, woff.data(), sizeof(long long) * woff.size(), cudaMemcpyHostToDevice, c.stream));
+  RH_CUDA(cudaStreamSynchronize(c.stream));  // the host vectors above are locals
   if (b.nwork > b.partial_cap) {
     cudaFree(b.d_partial);
     b.d_partial = nullptr;
-    RH_CUDA(cudaMalloc(&b.d_partial, sizeof(double) * 5 * b.nwork));
-    b.partial_cap = b.nwork;
+    const long long want = std::max(b.nwork, 2 * b.partial_cap);  // grow geometrically: fewer reallocations
+    RH_CUDA(cudaMalloc(&b.d_partial, sizeof(double) * 5 * want));
+    b.partial_cap = want;
+    if (b.graph) {  // the captured steps point at the old buffer
+      cudaGraphExecDestroy(b.graph);
+      b.graph = nullptr;
+    }
   }
   const BatchReg* reg = find_batch(b.precision, b.cfg.txo, b.cfg.tyo, b.cfg.minb, b.slope, b.riemann);
   if (!reg) {
@@ -336,13 +339,16 @@ int rebuild() {
               b.slope, b.riemann);
     return RH_EINVAL;
   }
-  RH_CUDA(cudaFuncSetAttribute(reg->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)reg->smem));
-  int per_sm = 0;
-  RH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reg->func, reg->threads, reg->smem));
-  b.nblocks = std::max(1, per_sm) * c.sm_count;
+  if (reg != b.occ_reg) {
+    RH_CUDA(cudaFuncSetAttribute(reg->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)reg->smem));
+    RH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b.occ_per_sm, reg->func, reg->threads, reg->smem));
+    b.occ_reg = reg;
+  }
+  b.nblocks = std::max(1, b.occ_per_sm) * c.sm_count;
   if (b.nwork > 0 && b.nwork < b.nblocks) b.nblocks = (int)b.nwork;
-  // graph of two steps (parity p, then 1-p), each: persistent kernel + reduction
-  if (b.graph) {
+  // graph of two steps (parity p, then 1-p), each: persistent kernel + reduction;
+  // an existing executable graph is updated in place when the topology allows
+  if (b.nslot == 0 && b.graph) {
     cudaGraphExecDestroy(b.graph);
     b.graph = nullptr;
   }
@@ -363,7 +369,17 @@ int rebuild() {
                                                          par);
     }
     RH_CUDA(cudaStreamEndCapture(c.stream, &g));
-    RH_CUDA(cudaGraphInstantiate(&b.graph, g, 0));
+    bool updated = false;
+    if (b.graph) {
+      cudaGraphExecUpdateResultInfo info;
+      updated = cudaGraphExecUpdate(b.graph, g, &info) == cudaSuccess;
+      if (!updated) {
+        cudaGetLastError();  // clear the update failure
+        cudaGraphExecDestroy(b.graph);
+        b.graph = nullptr;
+      }
+    }
+    if (!updated) RH_CUDA(cudaGraphInstantiate(&b.graph, g, 0));
     cudaGraphDestroy(g);
     b.graph_parity = b.parity;
   }
@@ -411,6 +427,8 @@ int rh_batch_init(int precision, int slope, int riemann, long long pool_octs) {
   RH_CUDA(cudaMalloc(&b.d_dt, sizeof(double) * b.cap));
   RH_CUDA(cudaMalloc(&b.d_t, sizeof(double) * b.cap));
   RH_CUDA(cudaMalloc(&b.d_tot, sizeof(double) * 5 * b.cap));
+  RH_CUDA(cudaMalloc(&b.d_order, sizeof(int) * b.cap));
+  RH_CUDA(cudaMalloc(&b.d_woff, sizeof(long long) * (b.cap + 1)));
   RH_CUDA(cudaMalloc(&b.d_counter, sizeof(unsigned long long)));
   RH_CUDA(cudaMemset(b.d_counter, 0, sizeof(unsigned long long)));
   RH_CUDA(cudaMemset(b.d_done, 0, sizeof(int) * b.cap));
