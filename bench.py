@@ -211,7 +211,8 @@ def bench_serve(args, rank, world, dist):
     """A serving session per GPU: make_requests(args.serve_requests) arriving
     as a Poisson stream at args.serve_rate per second (own seed per rank),
     continuous batching over a 16 GiB pool.  Reports time-to-solution
-    percentiles (rank 0's stream) and whole-job cell-updates/s."""
+    percentiles (rank 0's stream) and whole-job cell-updates/s, then the same
+    requests all due at once ("burst": the server's capacity)."""
     from ramses2_b200.ranks import max_over_ranks, sum_over_ranks
     from ramses2_b200.serve import HydroServer, make_requests
 
@@ -225,7 +226,17 @@ def bench_serve(args, rank, world, dist):
         if dist is not None:
             dist.barrier()
         st = srv.run(reqs, realtime=True)
+        # capacity: the same requests all due at once (closed loop)
+        burst = make_requests(args.serve_requests, rate_hz=args.serve_rate, seed=20261203 + rank)
+        if dist is not None:
+            dist.barrier()
+        sb = srv.run(burst, realtime=False)
         srv.close()
+        if dist is not None:
+            sb["cell_updates"] = sum_over_ranks([sb["cell_updates"]], dist)[0]
+            sb["makespan_s"] = max_over_ranks([sb["makespan_s"]], dist)[0]
+            sb["cell_updates_per_s"] = sb["cell_updates"] / sb["makespan_s"]
+        st["burst"] = {k: sb[k] for k in ("makespan_s", "cell_updates_per_s", "latency_p50_s", "latency_p99_s")}
         if dist is not None:
             st["cell_updates"] = sum_over_ranks([st["cell_updates"]], dist)[0]
             st["makespan_s"] = max_over_ranks([st["makespan_s"]], dist)[0]

@@ -6,12 +6,16 @@
  * __graft_entry__.smoke() and bench.py's cpu_baseline / reference legs may
  * load this library; the product path never links or calls it.
  *
- * Parity status: UNPINNED against the reference binary.  The reference path is
- * Fortran / CUDA Fortran and no Fortran compiler exists in the build image, and
- * the reference ships no golden vectors for this path.  The restatement is
- * pinned instead by known-answer physics (analytic Sedov solution generated
- * from the reference's own utils/py/sedov.py, exact conservation, symmetry,
- * translation/rotation invariance) — see tests/.
+ * Parity status: the Fortran reference binary cannot be built (no Fortran
+ * compiler in the image) and the reference ships no golden vectors for this
+ * path.  The restatement is pinned (a) against the reference's own code: its
+ * Metal port of the GPU hydro kernel (metal/kernels/hydro.metal, float32,
+ * mirroring gpu/gpu_hydro.cuf) compiles as C++ (oracle/Makefile target `ref`)
+ * and agrees with this oracle at FP32 rounding for the Riemann solvers, the
+ * per-oct trace + Riemann pipeline of every slope type and courant_fine; and
+ * (b) by known-answer physics (analytic Sedov solution from the reference's
+ * utils/py/sedov.py, exact conservation, symmetry, rotation invariance).
+ * FP64 bit-level agreement with the Fortran CPU path stays unverifiable here.
  *
  * Every function cites the reference file:line it restates.
  */
