@@ -78,6 +78,21 @@ int ref_msl_oct_fluxes(const float* u, float gamma, float smallr, float smallc2,
   return 0;
 }
 
+// One Godunov step of a level through the shader's hydro_integrator_kernel:
+// every oct is one threadgroup run by a single thread (the shader's loops take
+// the thread count as their stride, its barriers separate the phases).
+// unew must hold uold on entry; nbor is the shader's [ngridmax][27] table of
+// 1-based neighbour octs (x fastest).
+int ref_msl_godunov(const oct_t* grid, const float* uold, float* unew, const int* nbor, int head_idx, int noct,
+                    int ngridmax, int ilevel, int levelmin, int levelmax, float gamma, float smallr, float smallc2,
+                    float dt, float dx, int slope, int riemann, const float* grav, float smax_cap) {
+  for (int b = 0; b < noct; ++b)
+    hydro_integrator_kernel(grid, uold, unew, nbor, head_idx, noct, ngridmax, ilevel, levelmin, levelmax, gamma,
+                            smallr, smallc2, dt, dx, slope, riemann, grav, nullptr, nullptr, smax_cap, (uint)b, 0u,
+                            1u);
+  return 0;
+}
+
 // courant_fine of a level through the shader's cmpdt_kernel, run one thread at
 // a time (one-lane SIMD groups): out = (mass, ekin, eint, emag, dt).
 int ref_msl_cmpdt(const oct_t* grid, const float* uold, int head_idx, int num_octs, float dx, float gamma,

@@ -12,7 +12,8 @@
  * Metal port of the GPU hydro kernel (metal/kernels/hydro.metal, float32,
  * mirroring gpu/gpu_hydro.cuf) compiles as C++ (oracle/Makefile target `ref`)
  * and agrees with this oracle at FP32 rounding for the Riemann solvers, the
- * per-oct trace + Riemann pipeline of every slope type and courant_fine; and
+ * per-oct trace + Riemann pipeline of every slope type, courant_fine and a
+ * whole Godunov step of a periodic level; and
  * (b) by known-answer physics (analytic Sedov solution from the reference's
  * utils/py/sedov.py, exact conservation, symmetry, rotation invariance).
  * FP64 bit-level agreement with the Fortran CPU path stays unverifiable here.

@@ -8,7 +8,9 @@ into oracle/_ref/librh_ref_msl.so.  These tests feed identical inputs to the
 shader functions and to the oracle and require agreement at FP32 rounding:
 the three Riemann solvers, the per-oct trace + Riemann pipeline (ctoprim,
 slopes with the momentum bound, Hancock predictor, face states, rotations)
-for every slope type, and the courant_fine reduction.  Skipped where the
+for every slope type, the courant_fine reduction and a whole Godunov step of a periodic level
+(the shader's hydro_integrator_kernel: gather, trace, Riemann, conservative
+update).  Skipped where the
 shader library was not built (no reference checkout)."""
 import ctypes as C
 import os
@@ -33,6 +35,8 @@ def _lib():
                                      f32]
     L.ref_msl_cmpdt.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
                                 C.c_float, C.c_float, C.c_void_p, C.c_void_p]
+    L.ref_msl_godunov.argtypes = [C.c_void_p] * 4 + [C.c_int] * 6 + [C.c_float] * 5 + [C.c_int, C.c_int,
+                                                                                       C.c_void_p, C.c_float]
     return L
 
 
@@ -109,3 +113,48 @@ def test_courant_fine_matches_reference_shader():
     assert out[4] == pytest.approx(ref[4], rel=1e-6)   # dt
     assert out[0] == pytest.approx(ref[0], rel=2e-4)   # mass (float32 running sum of 32768 cells)
     assert out[1] == pytest.approx(ref[1], rel=2e-4)   # total energy
+
+
+@pytest.mark.parametrize("riemann", ["llf", "hll", "hllc"])
+@pytest.mark.parametrize("slope", [0, 1, 2])
+def test_godunov_step_matches_reference_shader(riemann, slope):
+    """One step of a periodic 16^3 level: oracle godunov_fine (FP64) vs the
+    shader's hydro_integrator_kernel (float32; one threadgroup per oct run by
+    one thread) fed the same float32-representable state and the shader's
+    27-neighbour table.  The new state agrees to float32 storage rounding and
+    the update (unew - uold) to float32 arithmetic."""
+    L = _lib()
+    lev, n, no, g = 4, 16, 8, 1.4
+    m = uniform_mesh(lev, bc="periodic")
+    zz, yy, xx = (np.indices((n, n, n)) + 0.5) / n
+    rho = 1 + 0.3 * np.sin(2 * np.pi * xx) * np.cos(2 * np.pi * yy) + 0.2 * np.sin(2 * np.pi * zz)
+    p = 1 + 0.5 * np.cos(2 * np.pi * (xx - zz))
+    m.from_dense(prim_to_cons(rho, 0.4 * np.sin(2 * np.pi * yy), -0.3 * np.cos(2 * np.pi * zz),
+                              0.2 * np.sin(2 * np.pi * (xx + yy)), p, g), lev)
+    m.uold[:] = _f32exact(m.uold)
+    ck = m.grid["ckey"].astype(np.int64)
+    idx = np.zeros((no, no, no), np.int64)
+    idx[ck[:, 0], ck[:, 1], ck[:, 2]] = np.arange(len(ck)) + 1
+    nbor = np.zeros((len(ck), 27), np.int32)
+    for t in range(27):
+        d = (t % 3 - 1, (t // 3) % 3 - 1, t // 9 - 1)
+        nbor[:, t] = idx[(ck[:, 0] + d[0]) % no, (ck[:, 1] + d[1]) % no, (ck[:, 2] + d[2]) % no]
+    P = HydroParams.make(gamma=g, courant_factor=0.8, slope_type=slope, riemann=riemann)
+    u0 = m.uold.copy()
+    o = oracle.OracleHydro(m, P)
+    dt = float(np.float32(0.5 * o.courant_fine(lev)[4]))
+    o.set_unew(lev)
+    o.godunov_fine(lev, dt)
+    ref = o.unew.copy()
+    u32 = np.ascontiguousarray(u0, np.float32)
+    un32 = u32.copy()
+    grav = np.zeros(3, np.float32)
+    dx = m.dx(lev)
+    L.ref_msl_godunov(m.grid.ctypes.data, u32.ctypes.data, un32.ctypes.data, nbor.ctypes.data, 1, len(ck), len(ck),
+                      lev, lev, lev, g, P.smallr, P.smallc ** 2, dt, dx, slope, {"llf": 1, "hll": 2, "hllc": 3}[riemann],
+                      grav.ctypes.data, 0.8 * dx / dt)
+    out = un32.astype(np.float64)
+    state = np.abs(out - ref).sum(axis=(0, 2)) / np.abs(ref).sum(axis=(0, 2))
+    update = np.abs(out - ref).sum(axis=(0, 2)) / np.abs(ref - u0).sum(axis=(0, 2))
+    assert np.all(state <= 2e-7), state
+    assert np.all(update <= 1e-4), update
