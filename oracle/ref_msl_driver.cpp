@@ -93,6 +93,16 @@ int ref_msl_godunov(const oct_t* grid, const float* uold, float* unew, const int
   return 0;
 }
 
+// Restriction of a fine level into its parents through the shader's
+// upload_kernel, one thread per fine oct; father[] holds the 1-based parent
+// oct of every oct.
+int ref_msl_upload(const oct_t* grid, const int* father, float* uold, int head_idx, int num_octs,
+                   int internal_energy, float gamma, float smallr, float smallc2) {
+  for (int t = 0; t < num_octs; ++t)
+    upload_kernel(grid, father, uold, head_idx, num_octs, internal_energy, gamma, smallr, smallc2, (uint)t);
+  return 0;
+}
+
 // courant_fine of a level through the shader's cmpdt_kernel, run one thread at
 // a time (one-lane SIMD groups): out = (mass, ekin, eint, emag, dt).
 int ref_msl_cmpdt(const oct_t* grid, const float* uold, int head_idx, int num_octs, float dx, float gamma,

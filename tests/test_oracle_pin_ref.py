@@ -8,9 +8,10 @@ into oracle/_ref/librh_ref_msl.so.  These tests feed identical inputs to the
 shader functions and to the oracle and require agreement at FP32 rounding:
 the three Riemann solvers, the per-oct trace + Riemann pipeline (ctoprim,
 slopes with the momentum bound, Hancock predictor, face states, rotations)
-for every slope type, the courant_fine reduction and a whole Godunov step of a periodic level
+for every slope type, the courant_fine reduction a whole Godunov step of a periodic level
 (the shader's hydro_integrator_kernel: gather, trace, Riemann, conservative
-update).  Skipped where the
+update), the restriction (upload_kernel) and the gradient flags
+(flag.metal's hydro_flag_kernel).  Skipped where the
 shader library was not built (no reference checkout)."""
 import ctypes as C
 import os
@@ -37,7 +38,22 @@ def _lib():
                                 C.c_float, C.c_float, C.c_void_p, C.c_void_p]
     L.ref_msl_godunov.argtypes = [C.c_void_p] * 4 + [C.c_int] * 6 + [C.c_float] * 5 + [C.c_int, C.c_int,
                                                                                        C.c_void_p, C.c_float]
+    L.ref_msl_upload.argtypes = [C.c_void_p] * 3 + [C.c_int] * 3 + [C.c_float] * 3
+    L.ref_msl_hydro_flag.argtypes = [C.c_void_p] * 3 + [C.c_int] * 2 + [C.c_float] * 7
     return L
+
+
+def _nbor27(m, no):
+    """The shader's neighbour table of a periodic complete level: 1-based
+    index of each of the 27 octs around an oct (x fastest)."""
+    ck = m.grid["ckey"].astype(np.int64)
+    idx = np.zeros((no, no, no), np.int64)
+    idx[ck[:, 0], ck[:, 1], ck[:, 2]] = np.arange(len(ck)) + 1
+    nbor = np.zeros((len(ck), 27), np.int32)
+    for t in range(27):
+        d = (t % 3 - 1, (t // 3) % 3 - 1, t // 9 - 1)
+        nbor[:, t] = idx[(ck[:, 0] + d[0]) % no, (ck[:, 1] + d[1]) % no, (ck[:, 2] + d[2]) % no]
+    return nbor
 
 
 def _f32exact(a):
@@ -132,13 +148,8 @@ def test_godunov_step_matches_reference_shader(riemann, slope):
     m.from_dense(prim_to_cons(rho, 0.4 * np.sin(2 * np.pi * yy), -0.3 * np.cos(2 * np.pi * zz),
                               0.2 * np.sin(2 * np.pi * (xx + yy)), p, g), lev)
     m.uold[:] = _f32exact(m.uold)
-    ck = m.grid["ckey"].astype(np.int64)
-    idx = np.zeros((no, no, no), np.int64)
-    idx[ck[:, 0], ck[:, 1], ck[:, 2]] = np.arange(len(ck)) + 1
-    nbor = np.zeros((len(ck), 27), np.int32)
-    for t in range(27):
-        d = (t % 3 - 1, (t // 3) % 3 - 1, t // 9 - 1)
-        nbor[:, t] = idx[(ck[:, 0] + d[0]) % no, (ck[:, 1] + d[1]) % no, (ck[:, 2] + d[2]) % no]
+    ck = m.grid["ckey"]
+    nbor = _nbor27(m, no)
     P = HydroParams.make(gamma=g, courant_factor=0.8, slope_type=slope, riemann=riemann)
     u0 = m.uold.copy()
     o = oracle.OracleHydro(m, P)
@@ -158,3 +169,56 @@ def test_godunov_step_matches_reference_shader(riemann, slope):
     update = np.abs(out - ref).sum(axis=(0, 2)) / np.abs(ref - u0).sum(axis=(0, 2))
     assert np.all(state <= 2e-7), state
     assert np.all(update <= 1e-4), update
+
+
+def test_hydro_flags_match_reference_shader():
+    """Gradient flags of a periodic level (every neighbour exists, where the
+    CPU and GPU reference flaggers coincide): same cells flagged."""
+    from ramses2_b200._abi import FlagParams
+
+    L = _lib()
+    rng = np.random.default_rng(21)
+    m = uniform_mesh(5, bc="periodic")
+    g, dense = riemann3d_state(rng, 32, gamma=1.4)
+    zz, yy, xx = (np.indices((32, 32, 32)) + 0.5) / 32
+    dense[0] *= 1 + 0.3 * np.sin(4 * np.pi * xx) * np.cos(2 * np.pi * yy) + 0.1 * zz
+    m.from_dense(dense, 5)
+    m.uold[:] = _f32exact(m.uold)
+    P = HydroParams.make(gamma=g)
+    ref = np.zeros((m.ngridmax, 8), np.int32)
+    n = oracle.OracleHydro(m, P).hydro_flag(5, FlagParams.make(err_grad_d=0.2, err_grad_p=0.3), ref)
+    out = np.zeros((m.ngridmax, 8), np.int32)
+    u32 = np.ascontiguousarray(m.uold, np.float32)
+    L.ref_msl_hydro_flag(out.ctypes.data, _nbor27(m, 16).ctypes.data, u32.ctypes.data, 1, int(m.noct[5]), g,
+                         P.smallr, P.smallc ** 2, 0.2, 0.3, 1e-10, 1e-10)
+    assert n > 0 and np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("ivar", [0, 1])
+def test_upload_matches_reference_shader(ivar):
+    from ramses2_b200.mesh import amr_mesh, fill_amr_prim
+
+    L = _lib()
+    m = amr_mesh(4, 6, lambda x, l: np.sqrt(((x - 0.52) ** 2).sum(-1)) < 0.16)
+
+    def prim(x, l):
+        r = np.sqrt(((x - 0.5) ** 2).sum(-1))
+        z = np.zeros_like(r)
+        return (1 + 0.5 * np.exp(-r ** 2 / 0.01), 0.3 + 0.2 * np.sin(6 * x[..., 1]), -0.2 + z, 0.1 + 0.1 * x[..., 0],
+                1 + 4 * np.exp(-r ** 2 / 0.004))
+
+    fill_amr_prim(m, prim, 1.4)
+    m.uold[:] = _f32exact(m.uold)
+    P = HydroParams.make(gamma=1.4, interpol_var=ivar)
+    u0 = m.uold.copy()
+    o = oracle.OracleHydro(m, P)
+    for lev in (5, 4):
+        o.upload_fine(lev)
+    ref = m.uold.copy()
+    key = {(int(r["lev"]), *map(int, r["ckey"])): i + 1 for i, r in enumerate(m.grid)}
+    father = np.array([key.get((int(r["lev"]) - 1, *(int(c) // 2 for c in r["ckey"])), 0) for r in m.grid], np.int32)
+    u32 = np.ascontiguousarray(u0, np.float32)
+    for lev in (6, 5):
+        L.ref_msl_upload(m.grid.ctypes.data, father.ctypes.data, u32.ctypes.data, int(m.head[lev]), int(m.noct[lev]),
+                         ivar, 1.4, P.smallr, P.smallc ** 2)
+    assert np.abs(u32 - ref).max() <= 2e-7 * np.abs(ref).max()
