@@ -9,6 +9,10 @@
  * gpu/gpu_runner.cuf:969,993); the Fortran shim turns a nonzero code into
  * mdl_abort.
  *
+ * The library keeps one context per process (one device, one stream, one
+ * resident mesh), as the reference drives its GPU from one host thread per
+ * MPI rank; calls from several host threads at once are not supported.
+ *
  * Host arrays keep the reference layout: uold(1:8,1:nvar,1:ngridmax) column
  * major (hydro/amr_commons.f90 mesh_t, amr/amr_commons.f90:811-920), i.e. oct
  * igrid occupies 8*nvar consecutive doubles at offset (igrid-1)*8*nvar, and

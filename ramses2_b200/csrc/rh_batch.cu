@@ -518,42 +518,57 @@ int rh_batch_add(const rh_batch_problem* p, const rh_batch_ic* ic, int* id) {
     set_error("rh_batch_add: pool full (%lld octs requested)", noct);
     return RH_ENOMEM;
   }
+  const BatchProb P = make_prob(*p, oct0);
+  const bool fp32 = b.precision == RH_PREC_FP32_BULK;
+  double* host_dev = nullptr;
+  // device set-up of the problem; on any failure the pool range and the slot
+  // are released again, so a failed add leaves the batch as it was
+  auto setup = [&]() -> cudaError_t {
+    cudaError_t e = cudaSuccess;
+    if (ic->kind == RH_IC_HOST) {
+      e = cudaMalloc(&host_dev, sizeof(double) * 40 * noct);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(host_dev, ic->host_uold, sizeof(double) * 40 * noct, cudaMemcpyHostToDevice, c.stream);
+      if (e != cudaSuccess) return e;
+    }
+    const long long ncell = noct * 8;
+    batch_ic_kernel<<<(unsigned)((ncell + 255) / 256), 256, 0, c.stream>>>(*ic, P, b.ud[b.parity], b.uf[b.parity],
+                                                                            fp32 ? 1 : 0, host_dev);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const long long nblk = (ncell + 255) / 256;
+    if (nblk > b.tmp_cap) {
+      cudaStreamSynchronize(c.stream);
+      cudaFree(b.d_tmp);
+      b.d_tmp = nullptr;
+      b.tmp_cap = 0;
+      if ((e = cudaMalloc(&b.d_tmp, sizeof(double) * 5 * nblk)) != cudaSuccess) return e;
+      b.tmp_cap = nblk;
+    }
+    batch_cfl_kernel<<<(unsigned)nblk, 256, 0, c.stream>>>(P, b.ud[b.parity], b.uf[b.parity], fp32 ? 1 : 0,
+                                                           b.d_tmp);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    batch_init_dt_kernel<<<1, 256, 0, c.stream>>>(P, slot, b.d_tmp, nblk, b.d_dt, b.d_tot);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const int zero = 0;
+    const double dz = 0.0;
+    if ((e = cudaMemcpyAsync(b.d_done + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, c.stream)) ||
+        (e = cudaMemcpyAsync(b.d_nstep + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, c.stream)) ||
+        (e = cudaMemcpyAsync(b.d_cur + slot, &b.parity, sizeof(int), cudaMemcpyHostToDevice, c.stream)) ||
+        (e = cudaMemcpyAsync(b.d_t + slot, &dz, sizeof(double), cudaMemcpyHostToDevice, c.stream)))
+      return e;
+    return cudaStreamSynchronize(c.stream);
+  };
+  const cudaError_t e = setup();
+  if (host_dev) cudaFree(host_dev);
+  if (e != cudaSuccess) {
+    free_octs(oct0, noct);
+    return cuda_fail(e, "rh_batch_add");
+  }
   HostProb& hp = b.probs[slot];
   hp.used = true;
   hp.p = *p;
   hp.oct0 = oct0;
   hp.noct = noct;
-  const BatchProb P = make_prob(*p, oct0);
-  const bool fp32 = b.precision == RH_PREC_FP32_BULK;
-  double* host_dev = nullptr;
-  if (ic->kind == RH_IC_HOST) {
-    RH_CUDA(cudaMalloc(&host_dev, sizeof(double) * 40 * noct));
-    RH_CUDA(cudaMemcpyAsync(host_dev, ic->host_uold, sizeof(double) * 40 * noct, cudaMemcpyHostToDevice, c.stream));
-  }
-  const long long ncell = noct * 8;
-  batch_ic_kernel<<<(unsigned)((ncell + 255) / 256), 256, 0, c.stream>>>(*ic, P, b.ud[b.parity], b.uf[b.parity],
-                                                                          fp32 ? 1 : 0, host_dev);
-  RH_CUDA(cudaGetLastError());
-  const long long nblk = (ncell + 255) / 256;
-  if (nblk > b.tmp_cap) {
-    cudaStreamSynchronize(c.stream);
-    cudaFree(b.d_tmp);
-    b.d_tmp = nullptr;
-    RH_CUDA(cudaMalloc(&b.d_tmp, sizeof(double) * 5 * nblk));
-    b.tmp_cap = nblk;
-  }
-  batch_cfl_kernel<<<(unsigned)nblk, 256, 0, c.stream>>>(P, b.ud[b.parity], b.uf[b.parity], fp32 ? 1 : 0, b.d_tmp);
-  RH_CUDA(cudaGetLastError());
-  batch_init_dt_kernel<<<1, 256, 0, c.stream>>>(P, slot, b.d_tmp, nblk, b.d_dt, b.d_tot);
-  RH_CUDA(cudaGetLastError());
-  const int zero = 0;
-  const double dz = 0.0;
-  RH_CUDA(cudaMemcpyAsync(b.d_done + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, c.stream));
-  RH_CUDA(cudaMemcpyAsync(b.d_nstep + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, c.stream));
-  RH_CUDA(cudaMemcpyAsync(b.d_cur + slot, &b.parity, sizeof(int), cudaMemcpyHostToDevice, c.stream));
-  RH_CUDA(cudaMemcpyAsync(b.d_t + slot, &dz, sizeof(double), cudaMemcpyHostToDevice, c.stream));
-  RH_CUDA(cudaStreamSynchronize(c.stream));
-  if (host_dev) cudaFree(host_dev);
   b.dirty = true;
   *id = slot;
   return RH_OK;

@@ -8,7 +8,8 @@ device pool (first fit, in arrival order), advances all admitted problems
 together (one persistent kernel launch per step, replayed from a CUDA graph),
 and retires a problem when it reaches t_end: its state is read back and its
 pool space is freed for the queue.  A request whose footprint exceeds the
-whole pool is rejected.  Latency is arrival -> result on the host.
+whole pool is rejected.  Latency is arrival -> result on the host (for a
+burst run, where every request is due at once, start of the run -> result).
 """
 import math
 import time
@@ -29,6 +30,7 @@ class Request:
     ic: object                 # rh_batch_ic
     kind: str = ""
     target_steps: int = 0
+    submitted: float = math.nan  # entered the server's queue (its arrival; 0 for a burst)
     admitted: float = math.nan
     finished: float = math.nan
     nsteps: int = 0
@@ -43,7 +45,7 @@ class Request:
 
     @property
     def latency(self):
-        return self.finished - self.arrival
+        return self.finished - self.submitted
 
 
 def initial_dt(states, gamma, dx, ndim, courant):
@@ -144,6 +146,7 @@ class HydroServer:
         while i < len(pending) or queue or active:
             tnow = now()
             while i < len(pending) and (not realtime or pending[i].arrival <= tnow):
+                pending[i].submitted = pending[i].arrival if realtime else 0.0
                 queue.append(pending[i])
                 i += 1
             # admission: first fit in arrival order
