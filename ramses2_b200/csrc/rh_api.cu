@@ -852,8 +852,8 @@ int rh_godunov(int head_idx, int num_subgrids, int ngridmax, int ilevel, int lev
     set_error("rh_godunov: need dt>0, dx>0, gamma>1, smallc2>0");
     return RH_EINVAL;
   }
-  if (slope < 0 || slope > 2) {
-    set_error("rh_godunov: slope_type %d not supported on this path (0, 1 or 2)", slope);
+  if (slope < 0 || slope > 3) {
+    set_error("rh_godunov: slope_type %d not supported (0 none, 1 minmod, 2 moncen, 3 positivity)", slope);
     return RH_EINVAL;
   }
   if (riemann < 1 || riemann > 3) {

@@ -52,7 +52,14 @@ template <> struct Store<float> {  // FP32-bulk: [oct][4][8] float + [oct][8] do
 };
 
 // T: storage element of the bulk variables; V: lane type of the arithmetic.
-template <typename T, typename V, int TXO, int TYO> struct Geo {
+// Slot of plane (or FP32-bulk layer) p >= -2 in a plane buffer of G::kNQ
+// entries, written out in place (a helper call changes the register
+// allocation of the pencil kernels).
+#define RH_QSLOT(G, p) ((G::kNQ == 2) ? ((p) & 1) : (((p) + 3) % 3))
+
+// NQ: primitive planes (or FP32-bulk oct layers) kept in shared memory: 2 for
+// slopes along the three axes, 3 for the 27-point limiter of slope_type 3.
+template <typename T, typename V, int TXO, int TYO, int NQ = 2> struct Geo {
   static constexpr int CX = 2 * TXO, CY = 2 * TYO;
   static constexpr int RW = CX + 2, RH = CY + 2;  // ring columns
   static constexpr int NRC = RW * RH;
@@ -66,7 +73,8 @@ template <typename T, typename V, int TXO, int TYO> struct Geo {
   static constexpr int NSTAGE = 2;
   static constexpr size_t kStageD = (size_t)NSTAGE * NSLOT * Store<T>::kSlotD * sizeof(double);
   static constexpr size_t kStageF = (size_t)NSTAGE * NSLOT * Store<T>::kSlotF * sizeof(float);
-  static constexpr size_t kQ = (size_t)2 * 5 * NLC * sizeof(V);
+  static constexpr size_t kQ = (size_t)NQ * 5 * NLC * sizeof(V);
+  static constexpr int kNQ = NQ;  // plane-buffer slot of plane (layer) p >= -2: RH_QSLOT(G, p)
   static constexpr size_t kFS = (size_t)10 * NRC * sizeof(V);
   static constexpr size_t kFX = (size_t)2 * 5 * NRC * sizeof(V);
   static constexpr size_t kRed = (size_t)NWARP * 4 * sizeof(double);

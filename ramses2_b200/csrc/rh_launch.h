@@ -25,7 +25,7 @@ int list_tiles(int prec, int amr, int* txo, int* tyo, int* minb, int max);
 
 template <int TXO, int TYO, int MINB, int SLOPE, int RIEMANN, bool AMR>
 cudaError_t launch_f64(const LevelArgs& A, const void* S, const void* H, int nblocks, cudaStream_t st) {
-  using G = Geo<double, double, TXO, TYO>;
+  using G = Geo<double, double, TXO, TYO, (SLOPE == 3 ? 3 : 2)>;
   auto k = godunov_pencil_kernel<double, TXO, TYO, MINB, SLOPE, RIEMANN, AMR>;
   static bool attr = false;
   if (!attr) {
@@ -40,7 +40,7 @@ cudaError_t launch_f64(const LevelArgs& A, const void* S, const void* H, int nbl
 
 template <int TXO, int TYO, int MINB, int SLOPE, int RIEMANN, bool AMR>
 cudaError_t launch_f32x2(const LevelArgs& A, const void* S, const void* H, int nblocks, cudaStream_t st) {
-  using G = Geo<float, float2, TXO, TYO>;
+  using G = Geo<float, float2, TXO, TYO, (SLOPE == 3 ? 3 : 2)>;
   auto k = godunov_pencil2_kernel<TXO, TYO, MINB, SLOPE, RIEMANN, AMR>;
   static bool attr = false;
   if (!attr) {
@@ -56,22 +56,22 @@ cudaError_t launch_f32x2(const LevelArgs& A, const void* S, const void* H, int n
 template <typename T, int TXO, int TYO, int MINB, bool AMR = false> struct TileRegistrar {
   TileRegistrar() {
     if constexpr (sizeof(T) == 8) {
-      using G = Geo<double, double, TXO, TYO>;
-#define RH_REG(S, R) \
-  register_launcher({RH_PREC_FP64, TXO, TYO, MINB, S, R, AMR}, &launch_f64<TXO, TYO, MINB, S, R, AMR>, G::kSmem, \
-                    G::NT);
+#define RH_REG(S, R)                                                                                              \
+  register_launcher({RH_PREC_FP64, TXO, TYO, MINB, S, R, AMR}, &launch_f64<TXO, TYO, MINB, S, R, AMR>,          \
+                    Geo<double, double, TXO, TYO, (S == 3 ? 3 : 2)>::kSmem, Geo<double, double, TXO, TYO>::NT);
       RH_REG(0, 1) RH_REG(0, 2) RH_REG(0, 3)
       RH_REG(1, 1) RH_REG(1, 2) RH_REG(1, 3)
       RH_REG(2, 1) RH_REG(2, 2) RH_REG(2, 3)
+      RH_REG(3, 1) RH_REG(3, 2) RH_REG(3, 3)
 #undef RH_REG
     } else {
-      using G = Geo<float, float2, TXO, TYO>;
-#define RH_REG(S, R) \
-  register_launcher({RH_PREC_FP32_BULK, TXO, TYO, MINB, S, R, AMR}, &launch_f32x2<TXO, TYO, MINB, S, R, AMR>, \
-                    G::kSmem, G::NT);
+#define RH_REG(S, R)                                                                                              \
+  register_launcher({RH_PREC_FP32_BULK, TXO, TYO, MINB, S, R, AMR}, &launch_f32x2<TXO, TYO, MINB, S, R, AMR>,   \
+                    Geo<float, float2, TXO, TYO, (S == 3 ? 3 : 2)>::kSmem, Geo<float, float2, TXO, TYO>::NT);
       RH_REG(0, 1) RH_REG(0, 2) RH_REG(0, 3)
       RH_REG(1, 1) RH_REG(1, 2) RH_REG(1, 3)
       RH_REG(2, 1) RH_REG(2, 2) RH_REG(2, 3)
+      RH_REG(3, 1) RH_REG(3, 2) RH_REG(3, 3)
 #undef RH_REG
     }
   }

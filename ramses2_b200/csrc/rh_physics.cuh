@@ -40,6 +40,23 @@ template <class V, int SLOPE> __device__ __forceinline__ V limited_slope(V qm1, 
   return vcopysign(vmin(dlim, vabs(dcen)), dcen);
 }
 
+// slope_type 3, the positivity-preserving 3D unsplit slope (umuscl.f90:
+// 2207-2269): the central differences of a variable, scaled by
+// min(1, min(|vmin - c|, |vmax - c|) / (|dfx| + |dfy| + |dfz|)/2) with vmin,
+// vmax the extremes of the 27-point neighbourhood (cell included; rounding is
+// monotone, so min(v - c) = min(v) - c exactly), so that the reconstruction
+// stays within the neighbourhood's range.
+template <class V> __device__ __forceinline__ void slope_posdef(V c, V vmn, V vmx, V dfx, V dfy, V dfz,
+                                                               const HydroK<V>& H, V& dx, V& dy, V& dz) {
+  const V one = H.two * H.half;
+  const V dff = H.half * (vabs(dfx) + vabs(dfy) + vabs(dfz));
+  const V lim = vmin(vabs(vmn - c), vabs(vmx - c));
+  const V slop = vsel(vgt(dff, H.zero), vmin(one, lim * vrcp(dff)), one);
+  dx = slop * dfx;
+  dy = slop * dfy;
+  dz = slop * dfz;
+}
+
 // Bound on the normal-velocity slope: rho*|dq|/2 <= rho_nbor*|u_nbor-u|.
 template <class V> __device__ __forceinline__ V momentum_bound(V dq, V rm1, V vm1, V v0, V rp1, V vp1, V ir0,
                                                                const HydroK<V>& H) {

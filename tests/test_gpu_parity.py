@@ -71,6 +71,24 @@ def test_one_step_fp64_solvers_slopes(riemann, slope):
     assert np.all(err <= TOL_FP64), err
 
 
+@pytest.mark.parametrize("bc,tile", [("outflow", (8, 8, 16)), ("periodic", (7, 7, 3)), ("reflexive", (8, 4, 2))])
+@pytest.mark.parametrize("riemann", ["llf", "hllc"])
+def test_slope_type3_fp64_and_fp32(bc, tile, riemann):
+    """slope_type 3, the positivity-preserving 27-point limiter
+    (umuscl.f90:2207-2269): FP64 <= 1e-12 per variable, FP32-bulk density
+    <= 1e-5 against the oracle."""
+    m = uniform_mesh(5, nsubgrid=1, bc=bc)
+    g = blast_state(m, 17, 1.4)
+    P = HydroParams.make(gamma=g, courant_factor=0.8, slope_type=3, riemann=riemann)
+    ref, out, (dto, _), (dtg, _) = run_one_step(m, P, tile=tile)
+    assert dtg == pytest.approx(dto, rel=1e-13)
+    err = rel_l1(out, ref)
+    assert np.all(err <= TOL_FP64), err
+    ref, out, _, _ = run_one_step(m, P, precision="fp32_bulk", tile=tile)
+    err = rel_l1(out, ref)
+    assert err[0] <= TOL_FP32_RHO, err
+
+
 @pytest.mark.parametrize("bc", ["outflow", "periodic", "reflexive",
                                 ["periodic", "periodic", "outflow", "outflow", "reflexive", "reflexive"]])
 @pytest.mark.parametrize("tile", [(7, 7, 3), (8, 4, 2), (8, 8, 16)])
@@ -238,10 +256,11 @@ def amr_step(solver, m, dt=None):
     return amr_coarse_step(solver, m, dt)
 
 
-@pytest.mark.parametrize("bc,itype,ivar", [("outflow", 1, 0), ("periodic", 2, 1), ("reflexive", 0, 0),
-                                           ("outflow", 3, 0)])
-def test_amr_steps_fp64(bc, itype, ivar):
+@pytest.mark.parametrize("bc,itype,ivar,slope", [("outflow", 1, 0, 2), ("periodic", 2, 1, 2), ("reflexive", 0, 0, 2),
+                                                 ("outflow", 3, 0, 2), ("outflow", 1, 0, 3)])
+def test_amr_steps_fp64(bc, itype, ivar, slope):
     m, P = amr_case(bc, itype, ivar)
+    P.slope_type = slope
     u0 = m.uold.copy()
     o = oracle.OracleHydro(m, P, nthreads=NTHREADS)
     dts = []
