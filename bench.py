@@ -258,6 +258,49 @@ def _timed(L, fn):
     return ms.value
 
 
+def bench_snapshot(L, m, prec, peak, reps=5):
+    """Restart / snapshot file images (include/ramses_hydro_io.h) of the
+    resident 256^3 state: device time of rh_file_image_device (CUDA events on
+    the library's stream) and wall time of rh_file_image into pinned host
+    memory.  Algorithmic bytes: state read once + image written once."""
+    import ctypes as C
+
+    from ramses2_b200._lib import check
+
+    noct = int(m.noct[LEVEL])
+    state_b = {"fp64": 320, "fp32_bulk": 192}[prec]
+    out = {}
+    for kind, name, rec in ((2, "hydro_backup", 320), (3, "hydro_output", 160)):
+        ptr, n = C.c_void_p(), C.c_longlong()
+        check(L.rh_file_image_device(kind, 1.4, C.byref(ptr), C.byref(n)), "rh_file_image_device")  # warm-up
+        ms = []
+        for _ in range(reps):
+            check(L.rh_timer_start(), "rh_timer_start")
+            check(L.rh_file_image_device(kind, 1.4, C.byref(ptr), C.byref(n)), "rh_file_image_device")
+            t = C.c_float()
+            check(L.rh_timer_stop(C.byref(t)), "rh_timer_stop")
+            ms.append(t.value)
+        dev_ms = float(np.median(ms))
+        gbs = noct * (state_b + rec) / (dev_ms * 1e-3) / 1e9
+        try:
+            import torch
+
+            host = torch.empty(int(n.value), dtype=torch.uint8, pin_memory=True)
+            hptr = host.data_ptr()
+        except Exception:
+            host = np.empty(int(n.value), np.uint8)
+            hptr = host.ctypes.data
+        got = C.c_longlong()
+        check(L.rh_file_image(kind, 1.4, C.c_void_p(hptr), n.value, C.byref(got)), "rh_file_image")
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            check(L.rh_file_image(kind, 1.4, C.c_void_p(hptr), n.value, C.byref(got)), "rh_file_image")
+        host_ms = (time.perf_counter() - t0) / reps * 1e3
+        out[name] = {"bytes": int(n.value), "device_ms": dev_ms, "device_GBps": gbs, "frac_of_hbm": gbs / peak,
+                     "to_pinned_host_ms": host_ms, "to_host_GBps": n.value / (host_ms * 1e-3) / 1e9}
+    return out
+
+
 def leaf_rel_l1(m, a, b):
     """Relative L1 (rho, mx, my, mz, E) over the leaf cells of every level."""
     num = np.zeros(5)
@@ -427,6 +470,7 @@ def run_ours(args):
     L = lib()
     results = {}
     kernel_ms = {}
+    snapshot = {}
     tuned = {}
     for prec in ("fp64", "fp32_bulk"):
         m.uold[:] = u0
@@ -446,6 +490,7 @@ def run_ours(args):
         gpu.push_uold()
         dt, _ = gpu.step_uniform()
         kernel_ms[prec] = kernel_time(gpu, args.steps, dt)
+        snapshot[prec] = bench_snapshot(L, m, prec, measured_peaks()[0])
         if prec == "fp32_bulk":
             # end to end through the ABI with host buffers (pinned)
             try:
@@ -609,6 +654,7 @@ def run_ours(args):
         "turbulence": turb,
         "batch": batch,
         "serve": serve,
+        "snapshot": snapshot,
         "gpu_launches": launches,
         "clocks": results[prec]["clocks"],
     }

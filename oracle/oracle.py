@@ -3,9 +3,11 @@
 The checker restates RAMSES II's FP64 CPU hydro step (hydro/umuscl.f90,
 hydro/godunov_utils.f90, hydro/godunov_fine.f90, hydro/courant_fine.f90).
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs use it.
-Parity status: unpinned against the reference binary (no Fortran compiler in
-the image, no golden vectors shipped by the reference); pinned by the
-known-answer tests in tests/.
+Parity status: the Fortran reference binary cannot be built (no Fortran
+compiler in the image) and ships no golden vectors for this path; the checker
+is pinned against the reference's own code (its Metal hydro and flag shaders
+compiled as C++, tests/test_oracle_pin_ref.py; its Python output reader,
+tests/test_files_host.py) and by known-answer tests.
 """
 import ctypes as C
 import os
@@ -46,6 +48,7 @@ def lib():
                                            P(C.c_int32), P(C.c_longlong)]
         L.rh_oracle_courant_fine.argtypes = [P(MeshDesc), P(HydroParams), C.c_int, P(C.c_double),
                                              P(C.c_double)]
+        L.rh_oracle_output_prims.argtypes = [P(C.c_double), C.c_longlong, C.c_double, P(C.c_float)]
         L.rh_oracle_last_error.restype = C.c_char_p
         _lib = L
     return _lib
@@ -85,6 +88,67 @@ def interpol_hydro(u1, interpol_var, interpol_type, smallr=1e-10):
     out = np.zeros((5, 8))
     _check(lib().rh_oracle_interpol_hydro(dptr(a), dptr(out), interpol_var, interpol_type, smallr))
     return out
+
+
+def output_prims(uold, gamma):
+    """output_hydro's float32 primitives (hydro/output_hydro.f90:86-140) of
+    uold (noct, 5, 8) -> (noct, 5, 8) float32 = (rho, u, v, w, p)."""
+    u = np.ascontiguousarray(uold, np.float64)
+    q = np.zeros(u.shape, np.float32)
+    _check(lib().rh_oracle_output_prims(dptr(u), u.shape[0], float(gamma), q.ctypes.data_as(C.POINTER(C.c_float))))
+    return q
+
+
+FILE_AMR, FILE_HYDRO_BACKUP, FILE_HYDRO_OUTPUT = 1, 2, 3
+
+
+def file_image(kind, uold, grid, head, noct, levelmin, levelmax, gamma=None):
+    """Bytes of one rank's amr or hydro file, restated from the writers:
+
+    * header: int32 ndim, [nvar,] levelmin, nlevelmax, noct(levelmin:nlevelmax)
+      (amr/output_amr.f90:702-707 backup_amr; hydro/output_hydro.f90:208-218
+      backup_hydro; amr/ramses_commons.f90:138-158 open_file);
+    * amr: per level, per oct (head(l) .. tail(l)): int32 ckey(1:3) and the
+      refined bits, bit ind-1 set for a refined cell (output_amr.f90:712-727);
+    * hydro backup: per oct float64 uold(1:8,1:5) (output_hydro.f90:223-237);
+    * hydro output: per oct float32 q(1:8,1:5) of output_prims
+      (output_hydro.f90:77-149).
+
+    uold (ngridmax, 5, 8); grid OCT_DTYPE records; head/noct indexed by level.
+    """
+    levels = range(levelmin, levelmax + 1)
+    hdr = [3] + ([] if kind == FILE_AMR else [5]) + [levelmin, levelmax] + [int(noct[l]) for l in levels]
+    parts = [np.asarray(hdr, "<i4").tobytes()]
+    for l in levels:
+        a, n = int(head[l]) - 1, int(noct[l])
+        if n == 0:
+            continue
+        if kind == FILE_AMR:
+            g = grid[a:a + n]
+            rec = np.zeros((n, 4), "<i4")
+            rec[:, :3] = g["ckey"]
+            rec[:, 3] = ((g["refined"] != 0).astype(np.int64) << np.arange(8)).sum(axis=1)
+            parts.append(rec.tobytes())
+        elif kind == FILE_HYDRO_BACKUP:
+            parts.append(np.ascontiguousarray(uold[a:a + n], "<f8").tobytes())
+        elif kind == FILE_HYDRO_OUTPUT:
+            parts.append(output_prims(uold[a:a + n], gamma).astype("<f4").tobytes())
+        else:
+            raise ValueError("unknown file kind %r" % (kind,))
+    return b"".join(parts)
+
+
+def restart_offsets(kind, levelmin, levelmax, noct):
+    """0-based byte offset of each level's first oct in a backup file, from
+    the restart reader's formulas (amr/init_refine_restart.f90:387,396, 1-based):
+    13 + 4*nlevel + 16*nskip (amr), 17 + 4*nlevel + 320*nskip (hydro)."""
+    nlev = levelmax - levelmin + 1
+    base, rec = (13, 16) if kind == FILE_AMR else (17, 8 * 8 * 5)
+    off, nskip = {}, 0
+    for l in range(levelmin, levelmax + 1):
+        off[l] = base + 4 * nlev + rec * nskip - 1
+        nskip += int(noct[l])
+    return off
 
 
 class OracleHydro:

@@ -1165,4 +1165,34 @@ int rh_oracle_courant_fine(const rh_mesh_desc* m, const rh_hydro_params* p, int 
   return 0;
 }
 
+// output_hydro, hydro/output_hydro.f90:86-140 (hydro only: no MHD field, no
+// non-thermal energies, no passive scalars), for noct octs of uold(1:8,1:5,:):
+// q(1:8,1:5,:) = real((dd, vx, vy, vz, pp), kind=4).  Expressions are
+// evaluated left to right as written (gfortran's order; x**2 is x*x) and
+// -ffp-contract=off keeps every product and sum separately rounded.
+int rh_oracle_output_prims(const double* uold, long long noct, double gamma, float* q) {
+  if ((!uold || !q) && noct > 0) { g_err = "null array"; return RH_EINVAL; }
+  for (long long o = 0; o < noct; ++o) {
+    const double* u = uold + (size_t)o * 40;
+    float* qo = q + (size_t)o * 40;
+    for (int ind = 0; ind < 8; ++ind) {
+      const double dd = u[ind];
+      const double vx = u[8 + ind] / dd;
+      const double vy = u[16 + ind] / dd;
+      const double vz = u[24 + ind] / dd;
+      const double ekin = 0.5 * dd * (vx * vx + vy * vy + vz * vz);
+      const double emag = 0.0, erad = 0.0;
+      const double etot = u[32 + ind];
+      const double pp = (gamma - 1) * (etot - ekin - emag - erad);
+      qo[ind] = (float)dd;
+      qo[8 + ind] = (float)vx;
+      qo[16 + ind] = (float)vy;
+      qo[24 + ind] = (float)vz;
+      qo[32 + ind] = (float)pp;
+    }
+  }
+  return 0;
+}
+
 }  // extern "C"
+

@@ -78,6 +78,10 @@ int rh_oracle_upload_fine(const rh_mesh_desc* m, const rh_hydro_params* p, int i
 int rh_oracle_hydro_flag(const rh_mesh_desc* m, const rh_hydro_params* p, const rh_flag_params* f, int ilevel,
                          const double* uold, int* flag1, long long* nflag);
 
+/* output_hydro's primitive variables (hydro/output_hydro.f90:86-140):
+ * q(1:8,1:5,1:noct) float32 = (rho, u, v, w, p) of uold(1:8,1:5,1:noct). */
+int rh_oracle_output_prims(const double* uold, long long noct, double gamma, float* q);
+
 #ifdef __cplusplus
 }
 #endif

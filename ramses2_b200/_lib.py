@@ -46,6 +46,12 @@ SIGNATURES = {
     "rh_timer_start": (_i, []),
     "rh_timer_stop": (_i, [_P(C.c_float)]),
     "rh_selftest_wait": (_i, [C.c_longlong]),
+    # restart / snapshot files (include/ramses_hydro_io.h)
+    "rh_file_size": (_i, [_i, _P(C.c_longlong)]),
+    "rh_file_image": (_i, [_i, _d, C.c_void_p, C.c_longlong, _P(C.c_longlong)]),
+    "rh_file_image_device": (_i, [_i, _d, _P(C.c_void_p), _P(C.c_longlong)]),
+    "rh_restore_hydro": (_i, [C.c_void_p, C.c_longlong]),
+    "rh_batch_file_image": (_i, [_i, _i, C.c_void_p, C.c_longlong, _P(C.c_longlong)]),
     # batch (include/ramses_hydro_batch.h)
     "rh_batch_init": (_i, [_i, _i, _i, C.c_longlong]),
     "rh_batch_free": (_i, []),

@@ -150,6 +150,25 @@ class Batch:
     def fetch_dense(self, pid):
         return octs_to_dense(self.fetch(pid), self.problems[pid][0])
 
+    def file_image(self, pid, kind):
+        """Bytes of a problem's amr / hydro_backup / hydro_output file (one
+        level 1 of n/2 octs per axis, row-major octs)."""
+        from .files import batch_image
+        return batch_image(pid, kind)
+
+    def write_output(self, pid, root, number, backup=False):
+        """output_NNNNN (or backup_NNNNN) directory of one problem under root;
+        returns its path.  The cell size dx is boxlen/2 (level 1)."""
+        from . import files
+        n, p = self.problems[pid]
+        st = self.status(pid)
+        noct = (n[0] // 2) * (n[1] // 2) * (n[2] // 2)
+        path = files.dir_name(root, number, backup)
+        info = files.info_txt(1, 1, noct, st["nstep"], 2.0 * p.dx, st["t"], p.gamma)
+        files.write_dir(path, self.file_image(pid, "amr"),
+                        self.file_image(pid, "hydro_backup" if backup else "hydro_output"), info, backup)
+        return path
+
     def set_tile(self, txo, tyo, minb, lz):
         check(self.L.rh_batch_set_tile(int(txo), int(tyo), int(minb), int(lz)), "rh_batch_set_tile")
 

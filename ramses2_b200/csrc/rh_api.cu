@@ -247,6 +247,7 @@ static void free_state() {
   c.d_scratch = nullptr;
   c.scratch_elems = 0;
   c.have_mesh = false;
+  free_image_buffer();
 }
 
 // Build the pencil tables of a complete (uniform) level (on the device:

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "ramses_hydro_batch.h"
+#include "ramses_hydro_io.h"
 #include "rh_batch.cuh"
 #include "rh_internal.h"
 
@@ -702,6 +703,46 @@ int rh_batch_fetch(int id, double* host_uold) {
       }
   }
   return RH_OK;
+}
+
+// A problem as a one-level mesh (level 1, n/2 octs per axis, row-major octs)
+// in the restart / snapshot layouts of include/ramses_hydro_io.h.
+int rh_batch_file_image(int id, int kind, void* host_buf, long long cap, long long* nbytes) {
+  Batch& b = B();
+  Context& c = ctx();
+  if (!b.inited || id < 0 || id >= b.cap || !b.probs[id].used || !nbytes) {
+    set_error("rh_batch_file_image: no problem %d", id);
+    return RH_EINVAL;
+  }
+  const HostProb& hp = b.probs[id];
+  RH_CUDA(cudaStreamSynchronize(c.stream));
+  int cur = 0;
+  RH_CUDA(cudaMemcpy(&cur, b.d_cur + id, sizeof(int), cudaMemcpyDeviceToHost));
+  ImageSrc s;
+  s.bulk = b.precision == RH_PREC_FP32_BULK;
+  s.ud = b.ud[cur] + hp.oct0 * (s.bulk ? 8 : 40);
+  s.uf = s.bulk ? b.uf[cur] + hp.oct0 * 32 : nullptr;
+  s.levelmin = s.levelmax = 1;
+  s.oct0.push_back(0);
+  s.noct.push_back(hp.noct);
+  s.nxo = hp.p.n[0] / 2;
+  s.nyo = hp.p.n[1] / 2;
+  s.nzo = hp.p.n[2] / 2;
+  if (kind != RH_FILE_AMR && kind != RH_FILE_HYDRO_BACKUP && kind != RH_FILE_HYDRO_OUTPUT) {
+    set_error("rh_batch_file_image: unknown kind %d", kind);
+    return RH_EINVAL;
+  }
+  const long long need = image_bytes(kind, s);
+  *nbytes = need;
+  if (!host_buf || cap < need) {
+    set_error("rh_batch_file_image: buffer of %lld bytes, the image needs %lld", cap, need);
+    return RH_EINVAL;
+  }
+  const void* d = nullptr;
+  long long n = 0;
+  int rc = build_image(kind, s, hp.p.gamma, &d, &n);
+  if (rc) return rc;
+  return image_to_host(d, n, host_buf, cap);
 }
 
 int rh_batch_bench(int nsteps, float* ms_per_step) {

@@ -106,4 +106,19 @@ int prolong_ghosts(int l, double smallr);
 // complete levels (rh_tables.cu)
 int build_complete_tables_device(int l, const TileCfg& cfg, LevelTables& T);
 
+// restart / snapshot file images (rh_io.cu)
+struct ImageSrc {
+  const double* ud = nullptr;  // FP64: [oct][5][8]; FP32-bulk: E [oct][8]
+  const float* uf = nullptr;   // FP32-bulk: [oct][4][8]
+  int bulk = 0;
+  int levelmin = 1, levelmax = 1;
+  std::vector<long long> oct0, noct;  // per level from levelmin: first oct (0-based) and count
+  const rh_oct* grid = nullptr;       // oct records (amr file); nullptr: one row-major box level
+  long long nxo = 1, nyo = 1, nzo = 1;
+};
+long long image_bytes(int kind, const ImageSrc& s);
+int build_image(int kind, const ImageSrc& s, double gamma, const void** dimage, long long* nbytes);
+int image_to_host(const void* dimage, long long nbytes, void* host_buf, long long cap);
+void free_image_buffer();
+
 }  // namespace rh

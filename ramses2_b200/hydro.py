@@ -8,6 +8,7 @@ meaning: ``courant_fine`` (r_courant_fine, hydro/courant_fine.f90:18-52),
 ABI (include/ramses_hydro.h) exactly as the Fortran shim would.
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -110,6 +111,31 @@ class GodunovGPU:
 
     def sync(self):
         check(self.L.rh_sync(), "rh_sync")
+
+    # ---- restart / snapshot files (include/ramses_hydro_io.h) -------------------
+    def file_image(self, kind):
+        """Bytes of the amr / hydro_backup / hydro_output file of the current state."""
+        from .files import context_image
+        return context_image(kind, self.params.gamma)
+
+    def write_output(self, root, number, time=0.0, nstep_coarse=0, backup=False):
+        """output_NNNNN (or backup_NNNNN) directory of the current state under
+        root, in the reference's layout; returns its path."""
+        from . import files
+        m = self.mesh
+        path = files.dir_name(root, number, backup)
+        info = files.info_txt(m.levelmin, m.levelmax, m.ngridmax, nstep_coarse, m.boxlen, time, self.params.gamma)
+        files.write_dir(path, self.file_image("amr"), self.file_image("hydro_backup" if backup else "hydro_output"),
+                        info, backup)
+        return path
+
+    def restore(self, hydro_backup):
+        """Restart: uold from a hydro backup image (bytes) or a backup directory."""
+        from . import files
+        if isinstance(hydro_backup, str):
+            with open(os.path.join(hydro_backup, "hydro.00001"), "rb") as f:
+                hydro_backup = f.read()
+        files.restore_hydro(hydro_backup)
 
     def set_tile(self, txo, tyo, lz, minb=None):
         """Pencil tile (txo x tyo octs, lz layers); minb defaults to the

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     names = []
-    for h in ("ramses_hydro.h", "ramses_hydro_ext.h", "ramses_hydro_batch.h"):
+    for h in ("ramses_hydro.h", "ramses_hydro_ext.h", "ramses_hydro_batch.h", "ramses_hydro_io.h"):
         p = os.path.join(ROOT, "include", h)
         if not os.path.exists(p):
             continue
