@@ -32,6 +32,14 @@ int rh_level_info(int ilevel, int* npencil, long long* table_entries);
  * table offsets (npencil) and oct table (entries: 0-based oct index per
  * (pencil, layer row, oct column), boundary-resolved) to the host. */
 int rh_level_table(int ilevel, int* phdr, long long* poff, int* tab, long long max_entries);
+/* Interpolated ghost octs of a coarse-fine level: per ghost the 7 level l-1
+ * source octs (0-based; father cell first, then -x,+x,-y,+y,-z,+z) with their
+ * cell | reflexive-flip bits << 3, and the father (oct, cell); returns the
+ * ghost count (arrays may be null to query it), negative on error. */
+int rh_level_ghosts(int ilevel, int* gsrc_oct, unsigned char* gsrc_cf, int* gfather, long long max_ghosts);
+/* Where rh_set_mesh builds coarse-fine tables: 1 on the device (default),
+ * 0 on the host (the reference builder the device one is tested against). */
+int rh_set_table_builder(int on_device);
 /* Device pointers of the current uold / unew buffers (FP64: *_d is
  * [oct][5][8]; FP32-bulk: *_f is [oct][4][8] float, *_d is [oct][8] energy). */
 int rh_state_ptrs(void** uold_d, void** uold_f, void** unew_d, void** unew_f);

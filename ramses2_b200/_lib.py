@@ -41,6 +41,8 @@ SIGNATURES = {
     "rh_list_tiles": (_i, [_i, _P(_i), _P(_i), _P(_i), _i]),
     "rh_level_info": (_i, [_i, _P(_i), _P(C.c_longlong)]),
     "rh_level_table": (_i, [_i, _P(_i), _P(C.c_longlong), _P(_i), C.c_longlong]),
+    "rh_level_ghosts": (_i, [_i, _P(_i), _P(C.c_ubyte), _P(_i), C.c_longlong]),
+    "rh_set_table_builder": (_i, [_i]),
     "rh_state_ptrs": (_i, [_P(C.c_void_p), _P(C.c_void_p), _P(C.c_void_p), _P(C.c_void_p)]),
     "rh_bench_godunov": (_i, [_i, _i, _d, _d, _d, _d, _d, _d, _i, _i, _P(C.c_float)]),
     "rh_timer_start": (_i, []),

@@ -501,20 +501,45 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
   for (int l = c.levelmin; l <= c.levelmax; ++l) c.nlevels_used += c.noct[l] > 0;
   const bool multi = c.nlevels_used > 1;
   c.levels.assign(c.levelmax + 1, LevelTables());
-  // coarse-fine levels: host tables first, they fix the number of ghost octs
+  // coarse-fine levels: tables first, they fix the number of ghost octs
   long long nghost = 0;
+  std::vector<std::pair<int2*, long long>> dev_gfather;  // device-built ghost fathers, per level
+  rh_oct* d_grid = nullptr;
+  auto drop_tables = [&]() {
+    for (auto& t : c.levels) free_tables(t);
+    c.levels.clear();
+    for (auto& f : dev_gfather) cudaFree(f.first);
+    cudaFree(d_grid);
+  };
   for (int l = c.levelmin; l <= c.levelmax; ++l) {
     if (c.noct[l] == 0) continue;
     const long long box = ((long long)c.box_nx[0] << (l - 1)) * ((long long)c.box_nx[1] << (l - 1)) *
                           ((long long)c.box_nx[2] << (l - 1));
     if ((long long)c.noct[l] == box) continue;
-    rc = build_amr_tables(l, c.amr_cfg, (long long)c.ngridmax + nghost);
+    const long long gbase = (long long)c.ngridmax + nghost;
+    if (c.table_builder) {
+      cudaError_t e = cudaSuccess;
+      if (!d_grid) {
+        e = cudaMalloc(&d_grid, sizeof(rh_oct) * c.grid.size());
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(d_grid, c.grid.data(), sizeof(rh_oct) * c.grid.size(), cudaMemcpyHostToDevice,
+                              c.stream);
+      }
+      int2* gf = nullptr;
+      rc = e == cudaSuccess ? build_amr_tables_device(l, c.amr_cfg, gbase, d_grid, &gf)
+                            : cuda_fail(e, "oct records to the device");
+      if (gf) dev_gfather.push_back({gf, gbase});
+    } else {
+      rc = build_amr_tables(l, c.amr_cfg, gbase);
+    }
     if (rc) {
-      c.levels.clear();
+      drop_tables();
       return rc;
     }
     nghost += c.levels[l].nghost;
   }
+  cudaFree(d_grid);
+  d_grid = nullptr;
   c.nstate = (long long)c.ngridmax + nghost;
   const long long n = c.nstate;
   for (int i = 0; i < 2; ++i) {
@@ -536,6 +561,17 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
     RH_CUDA(cudaMalloc(&c.d_refmask, (size_t)n));
     RH_CUDA(cudaMemcpy(c.d_refmask, ref.data(), (size_t)n, cudaMemcpyHostToDevice));
     RH_CUDA(cudaMalloc(&c.d_gfather, sizeof(int2) * (size_t)std::max(1LL, nghost)));
+    int nlev_ghost = 0;
+    for (int l = c.levelmin; l <= c.levelmax; ++l) {
+      const LevelTables& T = c.levels[l];
+      if (!T.built || T.nghost == 0) continue;
+      const auto& f = dev_gfather[(size_t)nlev_ghost++];
+      RH_CUDA(cudaMemcpyAsync(c.d_gfather + (f.second - c.ngridmax), f.first, sizeof(int2) * T.nghost,
+                              cudaMemcpyDeviceToDevice, c.stream));
+    }
+    RH_CUDA(cudaStreamSynchronize(c.stream));
+    for (auto& f : dev_gfather) cudaFree(f.first);
+    dev_gfather.clear();
   }
   c.cur = 0;
   c.unew_pending.assign(c.levelmax + 1, 0);
@@ -549,6 +585,7 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
   if (rc) return rc;
   for (int l = c.levelmin; l <= c.levelmax; ++l) {
     if (c.noct[l] == 0) continue;
+    if (c.levels[l].built) continue;  // coarse-fine level built on the device
     if (c.levels[l].nghost > 0 || (c.levels[l].npencil > 0 && !c.levels[l].complete)) {
       rc = upload_amr_tables(l);
       if (rc) return rc;
@@ -974,6 +1011,36 @@ int rh_level_table(int ilevel, int* phdr, long long* poff, int* tab, long long m
     RH_CUDA(cudaMemcpyAsync(tab, T.d_ptab, sizeof(int) * T.ntab, cudaMemcpyDeviceToHost, c.stream));
     RH_CUDA(cudaStreamSynchronize(c.stream));
   }
+  return RH_OK;
+}
+
+int rh_level_ghosts(int ilevel, int* gsrc_oct, unsigned char* gsrc_cf, int* gfather, long long max_ghosts) {
+  int rc = check_ready();
+  if (rc) return -rc;
+  Context& c = ctx();
+  if (ilevel < 0 || ilevel > c.levelmax || !c.levels[ilevel].built) {
+    set_error("rh_level_ghosts: level %d has no tables", ilevel);
+    return -RH_EINVAL;
+  }
+  const LevelTables& T = c.levels[ilevel];
+  const long long n = T.nghost;
+  if ((gsrc_oct || gsrc_cf || gfather) && max_ghosts < n) {
+    set_error("rh_level_ghosts: %lld ghosts do not fit in %lld", n, max_ghosts);
+    return -RH_EINVAL;
+  }
+  if (n > 0) {
+    if (gsrc_oct) RH_CUDA(cudaMemcpy(gsrc_oct, T.d_gsrc_oct, sizeof(int) * 7 * n, cudaMemcpyDeviceToHost));
+    if (gsrc_cf) RH_CUDA(cudaMemcpy(gsrc_cf, T.d_gsrc_cf, 7 * n, cudaMemcpyDeviceToHost));
+    if (gfather)
+      RH_CUDA(cudaMemcpy(gfather, c.d_gfather + (T.gbase - c.ngridmax), sizeof(int2) * n, cudaMemcpyDeviceToHost));
+  }
+  return (int)n;
+}
+
+int rh_set_table_builder(int on_device) {
+  int rc = check_ready(false);
+  if (rc) return rc;
+  ctx().table_builder = on_device ? 1 : 0;
   return RH_OK;
 }
 

@@ -55,6 +55,7 @@ struct LevelTables {
 struct Context {
   bool inited = false;
   TileCfg amr_cfg{8, 4, 2, 8};  // tiles of multi-level meshes (coarse-fine kernels)
+  int table_builder = 1;        // coarse-fine tables: 1 on the device, 0 on the host
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
@@ -103,6 +104,9 @@ Context& ctx();
 int build_amr_tables(int l, const TileCfg& cfg, long long gbase);
 int upload_amr_tables(int l);
 int prolong_ghosts(int l, double smallr);
+// coarse-fine levels built on the device (rh_amr_tables.cu): same tables as
+// build_amr_tables; *d_gfather_out receives the level's ghost fathers (device)
+int build_amr_tables_device(int l, const TileCfg& cfg, long long gbase, const rh_oct* d_grid, int2** d_gfather_out);
 // complete levels (rh_tables.cu)
 int build_complete_tables_device(int l, const TileCfg& cfg, LevelTables& T);
 
