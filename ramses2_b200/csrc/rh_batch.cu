@@ -153,7 +153,7 @@ __global__ void batch_cfl_kernel(BatchProb P, const double* ud, const float* uf,
     }
     acc.add(r, m1, m2, m3, E, A);
   }
-  double v[4] = {acc.mass, acc.ekin, acc.eint, acc.dt};
+  double v[4] = {acc.mass, acc.ekin, acc.eint, acc.dt(A.cfl)};
   for (int off = 16; off > 0; off >>= 1) {
     v[0] += __shfl_down_sync(0xffffffffu, v[0], off);
     v[1] += __shfl_down_sync(0xffffffffu, v[1], off);

@@ -177,8 +177,14 @@ constexpr long long kWaitBound = 1ll << 22;  // bounded mbarrier spin (seconds a
 
 // Per-thread FP64 CFL / conserved-total accumulation of one new cell
 // (courant_fine.f90:317-386 + cmpdt).
+// Per-thread courant_fine accumulators.  The cell time step of cmpdt
+// (godunov_utils.f90:228-333) is a decreasing function of the cell's summed
+// signal speed ctot (dx-scaled constant over ctot, or its gravity form), so
+// the thread keeps the largest ctot and converts it once: min over cells of
+// dt(ctot) = dt(max ctot), with no division or square root of the dt formula
+// per cell.
 struct CflAcc {
-  double mass = 0, ekin = 0, eint = 0, dt = 1e300;
+  double mass = 0, ekin = 0, eint = 0, cmax = 0;
   __device__ __forceinline__ void add(double r, double m1, double m2, double m3, double E, const LevelArgs& A) {
     mass += r * A.vol;
     ekin += E * A.vol;
@@ -189,14 +195,39 @@ struct CflAcc {
     ei -= 0.5 * (m2 * m2) * irm * A.vol;
     ei -= 0.5 * (m3 * m3) * irm * A.vol;
     eint += ei;
-    const double d = cmpdt_cell(r, m1, m2, m3, E, A.cfl);
-    dt = d < dt ? d : dt;
+    const CflConst& C = A.cfl;
+    const double u = m1 * irm, v = m2 * irm, w = m3 * irm;
+    double e = E - 0.5 * rm * (u * u);
+    e = e - 0.5 * rm * (v * v);
+    e = e - 0.5 * rm * (w * w);
+    double p = C.gm1 * e;
+    const double pf = rm * C.smallp;
+    p = p > pf ? p : pf;
+    const double c = vsqrt(C.gamma * p * irm);
+    double ctot = fabs(u) + c;
+    if (C.ndim > 1) ctot += fabs(v) + c;
+    if (C.ndim > 2) ctot += fabs(w) + c;
+    cmax = ctot > cmax ? ctot : cmax;
+  }
+  // smallest cell dt of the accumulated cells (1e300 when there were none)
+  __device__ __forceinline__ double dt(const CflConst& C) const {
+    if (!(cmax > 0.0)) return 1e300;
+    double d;
+    if (C.gsum_dx == 0.0) {
+      d = C.k0 / cmax;
+    } else {
+      double grav = C.gsum_dx / (cmax * cmax);
+      grav = grav > 0.0001 ? grav : 0.0001;
+      d = C.two_cdx / (cmax * (1.0 + sqrt(1.0 + C.two_c * grav)));
+    }
+    return d < C.cdx_smallc ? d : C.cdx_smallc;
   }
 };
 
 // Deterministic block reduction of the CFL accumulators into the pencil partial.
-template <int NWARP> __device__ __forceinline__ void cfl_block_reduce(const CflAcc& a, double* red, double* out) {
-  double v[4] = {a.mass, a.ekin, a.eint, a.dt};
+template <int NWARP>
+__device__ __forceinline__ void cfl_block_reduce(const CflAcc& a, const CflConst& C, double* red, double* out) {
+  double v[4] = {a.mass, a.ekin, a.eint, a.dt(C)};
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
     v[0] += __shfl_down_sync(0xffffffffu, v[0], off);

@@ -66,12 +66,10 @@ __device__ __forceinline__ float2 operator-(float2 a) { return make_float2(-a.x,
 __device__ __forceinline__ float2 operator-(float2 a, float2 b) { return __fadd2_rn(a, -b); }
 __device__ __forceinline__ float2 operator*(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 vmin(float2 a, float2 b) {
-  return make_float2(a.x < b.x ? a.x : b.x, a.y < b.y ? a.y : b.y);
-}
-__device__ __forceinline__ float2 vmax(float2 a, float2 b) {
-  return make_float2(a.x > b.x ? a.x : b.x, a.y > b.y ? a.y : b.y);
-}
+// Fortran MIN / MAX of ordered (NaN-free) operands as one FMNMX per lane;
+// the results differ from a compare-and-select at most in the sign of a zero.
+__device__ __forceinline__ float2 vmin(float2 a, float2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
+__device__ __forceinline__ float2 vmax(float2 a, float2 b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
 __device__ __forceinline__ float2 vabs(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
 __device__ __forceinline__ float2 vcopysign(float2 a, float2 b) {
   return make_float2(copysignf(a.x, b.x), copysignf(a.y, b.y));
