@@ -40,8 +40,16 @@ class Request:
 
     @property
     def cells(self):
+        """Cells held on the device (a 2D problem: its two-cell-deep z slab)."""
         n = self.prob.n
         return int(n[0]) * int(n[1]) * int(n[2])
+
+    @property
+    def solved_cells(self):
+        """Cells of the problem as posed: nx*ny for a 2D request, whose
+        device slab holds each cell twice (identical z planes)."""
+        n = self.prob.n
+        return int(n[0]) * int(n[1]) * (int(n[2]) if int(self.prob.ndim) == 3 else 1)
 
     @property
     def latency(self):
@@ -178,7 +186,7 @@ class HydroServer:
                         r.result = b.fetch(pid)
                     b.remove(pid)
                     r.finished = now()
-                    updates += r.cells * r.nsteps
+                    updates += r.solved_cells * r.nsteps
                     if log:
                         log("req %d %s %s done: %d steps, latency %.3f s" % (r.rid, r.kind, tuple(r.prob.n),
                                                                              r.nsteps, r.latency))
