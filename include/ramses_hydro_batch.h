@@ -79,6 +79,12 @@ int rh_batch_list_tiles(int precision, int* txo, int* tyo, int* minb, int max);
 int rh_batch_bench(int nsteps, float* ms_per_step);
 /* Cells updated by one batch step over the unfinished problems. */
 long long rh_batch_cells(void);
+/* Kernel path of 2D problems (ndim 2: one z oct layer, periodic z): 1 (the
+ * default) the plane tile body, which does the x/y work once per cell and
+ * writes both planes; 0 the 3D pencil body.  Both give the same result bit for
+ * bit (the pencil body's z terms are exact zeros there); the choice is kept for
+ * that comparison. */
+int rh_batch_set_plane_path(int on);
 
 #ifdef __cplusplus
 }

@@ -69,6 +69,7 @@ SIGNATURES = {
     "rh_batch_list_tiles": (_i, [_i, _P(_i), _P(_i), _P(_i), _i]),
     "rh_batch_bench": (_i, [_i, _P(C.c_float)]),
     "rh_batch_cells": (C.c_longlong, []),
+    "rh_batch_set_plane_path": (_i, [_i]),
 }
 
 

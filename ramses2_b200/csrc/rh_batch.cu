@@ -73,6 +73,7 @@ struct Batch {
   bool dirty = true;             // work list / graph must be rebuilt
   const void* occ_reg = nullptr; // kernel whose occupancy occ_per_sm holds
   int occ_per_sm = 0;
+  int plane2d = 1;               // 2D problems on the plane tile body
   cudaGraphExec_t graph = nullptr;
   int graph_parity = 0;
   int nblocks = 0;
@@ -359,7 +360,8 @@ int rebuild() {
     for (int h = 0; h < 2; ++h) {
       const int par = (b.parity + h) & 1;
       BatchArgs A{b.d_prob, b.d_order, b.d_woff, b.nslot, b.nwork, b.cfg.txo, b.cfg.tyo, b.cfg.lz, b.d_counter,
-                  b.d_done, b.d_dt, b.d_partial, {b.ud[0], b.ud[1]}, {b.uf[0], b.uf[1]}, c.d_err};
+                  b.d_done, b.d_dt, b.d_partial, {b.ud[0], b.ud[1]}, {b.uf[0], b.uf[1]}, c.d_err,
+                  b.plane2d};
       cudaError_t e = reg->fn(A, par, b.nblocks, c.stream);
       if (e != cudaSuccess) {
         cudaStreamEndCapture(c.stream, &g);
@@ -605,6 +607,17 @@ int rh_batch_set_tile(int txo, int tyo, int minb, int lz) {
   return RH_OK;
 }
 
+int rh_batch_set_plane_path(int on) {
+  Batch& b = B();
+  if (!b.inited) {
+    set_error("rh_batch_init has not been called");
+    return RH_ESTATE;
+  }
+  b.plane2d = on ? 1 : 0;
+  b.dirty = true;
+  return RH_OK;
+}
+
 int rh_batch_step(int nsteps) {
   Batch& b = B();
   Context& c = ctx();
@@ -626,7 +639,8 @@ int rh_batch_step(int nsteps) {
       done_steps += 2;
     } else {
       BatchArgs A{b.d_prob, b.d_order, b.d_woff, b.nslot, b.nwork, b.cfg.txo, b.cfg.tyo, b.cfg.lz, b.d_counter,
-                  b.d_done, b.d_dt, b.d_partial, {b.ud[0], b.ud[1]}, {b.uf[0], b.uf[1]}, c.d_err};
+                  b.d_done, b.d_dt, b.d_partial, {b.ud[0], b.ud[1]}, {b.uf[0], b.uf[1]}, c.d_err,
+                  b.plane2d};
       RH_CUDA(reg->fn(A, b.parity, b.nblocks, c.stream));
       batch_reduce_kernel<<<b.nslot, 256, 0, c.stream>>>(b.d_prob, b.d_order, b.d_woff, b.d_partial, b.d_done,
                                                          b.d_nstep, b.d_cur, b.d_dt, b.d_t, b.d_tot, b.d_counter,

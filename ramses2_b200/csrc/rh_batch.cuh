@@ -3,6 +3,7 @@
 #pragma once
 #include "rh_godunov.cuh"
 #include "rh_godunov2.cuh"
+#include "rh_plane2d.cuh"
 
 namespace rh {
 
@@ -36,6 +37,7 @@ struct BatchArgs {
   double* ud[2];            // FP64 pool [oct][5][8], or FP32-bulk energy [oct][8]
   float* uf[2];             // FP32-bulk pool [oct][4][8]
   int* err;
+  int plane2d;              // 2D problems take the plane tile body (else the pencil body)
 };
 
 __device__ __forceinline__ int batch_slot(const long long* woff, int nslot, long long w) {
@@ -125,12 +127,23 @@ __device__ __noinline__ void batch_pencil(int rbase) {
   }
 }
 
+// One XY tile of a 2D problem (rh_plane2d.cuh), out of line like batch_pencil.
+template <typename T, int TXO, int TYO, int SLOPE, int RIEMANN>
+__device__ __noinline__ void batch_plane() {
+  const int4 hdr = rh_b_hdr;
+  if constexpr (sizeof(T) == 8) {
+    plane2d_body<T, double, TXO, TYO, SLOPE, RIEMANN>(rh_bA, rh_bS64, rh_bH64, hdr, rh_b_out);
+  } else {
+    plane2d_body<T, float2, TXO, TYO, SLOPE, RIEMANN>(rh_bA, rh_bS32, rh_bH32, hdr, rh_b_out);
+  }
+}
+
 template <typename T, typename V, int TXO, int TYO, int MINB, int SLOPE, int RIEMANN>
 __global__ void __launch_bounds__(Geo<T, V, TXO, TYO>::NT, MINB) batch_step_kernel(const BatchArgs B, int parity) {
   using G = Geo<T, V, TXO, TYO>;
   static_assert(G::NSLOT <= kBatchMaxSlots, "tile too wide for the dense offset table");
   __shared__ long long s_w;
-  __shared__ int s_skip;
+  __shared__ int s_skip, s_plane;
   if (threadIdx.x == 0) {
     rh_s_abort = 0;
     uint64_t* bar = reinterpret_cast<uint64_t*>(rh_smem + G::oBar);
@@ -157,6 +170,7 @@ __global__ void __launch_bounds__(Geo<T, V, TXO, TYO>::NT, MINB) batch_step_kern
           const int bz = (int)(li / ((long long)P.tx * P.ty));
           const int nzo = P.ncz >> 1;
           rh_b_hdr = make_int4(bx * B.txo, by * B.tyo, bz * B.lz, min(B.lz, nzo - bz * B.lz));
+          s_plane = B.plane2d && P.ndim == 2 && nzo == 1 && P.periodic[2];
           batch_level(P, dt, B.err, rh_bA);
           if constexpr (sizeof(T) == 8) {
             rh_bS64.uold_d = B.ud[parity] + P.oct0 * 40;
@@ -177,6 +191,10 @@ __global__ void __launch_bounds__(Geo<T, V, TXO, TYO>::NT, MINB) batch_step_kern
     __syncthreads();
     if (s_w >= B.nwork) break;
     if (s_skip) continue;
+    if (s_plane) {
+      batch_plane<T, TXO, TYO, SLOPE, RIEMANN>();
+      continue;
+    }
     {
       // oct index of (row, slot) = tab[NSLOT + row] + tab[slot], boundary-mapped
       const int4 hdr = rh_b_hdr;

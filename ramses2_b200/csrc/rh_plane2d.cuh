@@ -1,0 +1,189 @@
+// rh_plane2d.cuh — one XY tile of a plane (2D) batch problem.
+//
+// A 2D problem of the batch is stored as one z oct layer with periodic z, so
+// both cell planes of every oct hold the same values.  On such a problem the
+// pencil body's z work is exact zeros: every z slope is +0 (the z neighbours
+// equal the cell), the normal-velocity bound of a zero slope is +0, and the two
+// z faces of a plane see the same Riemann problem, so their flux difference is
+// +0.  This tile body does the x/y work only, with the same operations in the
+// same order as the pencil body (trace_cell with zero z slopes; the update adds
+// the +0 z difference as the pencil body does), and writes the result to both
+// planes: it matches the pencil body on such problems bit for bit, the
+// reference's 2D predictor (hydro/umuscl.f90:487-853 trace2d) being trace3d
+// without its z terms.  The CFL accumulators take each cell twice (both
+// planes), as the pencil body does.
+//
+// No staging: the tile's (2 TXO + 4) x (2 TYO + 4) cells are read straight from
+// the pool (a 2D tile is one layer, nothing to pipeline), converted to
+// primitives into the plane buffer, then traced, solved and updated by the
+// ring-column threads of the pencil geometry.
+#pragma once
+#include "rh_godunov.cuh"
+#include "rh_godunov2.cuh"
+
+namespace rh {
+
+__device__ __forceinline__ int plane_oct(int v, int n, int periodic) {
+  if (periodic) return ((v % n) + n) % n;
+  return v < 0 ? 0 : (v >= n ? n - 1 : v);
+}
+
+template <typename T, typename V, int TXO, int TYO, int SLOPE, int RIEMANN>
+__device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs<T>& S, const HydroK<V>& H,
+                                             const int4 hdr, double* out) {
+  constexpr bool F64 = sizeof(T) == 8;
+  using G = Geo<T, V, TXO, TYO>;
+  V* Q = reinterpret_cast<V*>(rh_smem + G::oQ);  // [5][NLC] primitives, then [NLC] 1/rho
+  V* IR = Q + 5 * G::NLC;
+  V* FS = reinterpret_cast<V*>(rh_smem + G::oFS);   // [10][NRC]: qp_x(5), qp_y(5)
+  V* FXY = reinterpret_cast<V*>(rh_smem + G::oFX);  // [2][5][NRC]: x then y fluxes
+  double* red = reinterpret_cast<double*>(rh_smem + G::oRed);
+  const int t = threadIdx.x;
+  const int ox0 = hdr.x, oy0 = hdr.y;
+  const int nxo = A.ncx >> 1, nyo = A.ncy >> 1;
+
+  // (A) primitives of every cell of the tile and its two-cell halo (plane a)
+  for (int i = t; i < G::NLC; i += G::NT) {
+    const int gx = 2 * ox0 - 2 + i % G::LW, gy = 2 * oy0 - 2 + i / G::LW;
+    const CellMap mx = map_coord(gx, A.ncx, A.periodic[0], A.btype[0], A.btype[1]);
+    const CellMap my = map_coord(gy, A.ncy, A.periodic[1], A.btype[2], A.btype[3]);
+    const int oct = plane_oct(gx >> 1, nxo, A.periodic[0]) + nxo * plane_oct(gy >> 1, nyo, A.periodic[1]);
+    const int c = mx.parity + 2 * my.parity;
+    V q[5], ir;
+    if constexpr (F64) {
+      double U[5];
+      ctoprim_f64(S.uold_d + (size_t)oct * 40, c, mx.flip, my.flip, false, H, q, ir, U);
+    } else {
+      float2 U[4];
+      double E[2];
+      ctoprim_f32x2(S.uold_f + (size_t)oct * 32, S.uold_d + (size_t)oct * 8, c, c + 4, mx.flip, my.flip, false, H,
+                    A.gm1_d, A.smalle_d, q, ir, U, E);
+    }
+#pragma unroll
+    for (int n = 0; n < 5; ++n) Q[n * G::NLC + i] = q[n];
+    IR[i] = ir;
+  }
+  __syncthreads();
+
+  Columns<G> col;
+  col.init(t, ox0, oy0, A);
+  const bool active = t < G::NRC;
+  V qmx[5], qmy[5];
+  // (C) slopes, predictor and x/y interface states of the ring cells
+  if (active) {
+    V cur[5], xm[5], xp[5], ym[5], yp[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      cur[n] = Q[n * G::NLC + col.lc];
+      xm[n] = Q[n * G::NLC + col.lc - 1];
+      xp[n] = Q[n * G::NLC + col.lc + 1];
+      ym[n] = Q[n * G::NLC + col.lc - G::LW];
+      yp[n] = Q[n * G::NLC + col.lc + G::LW];
+    }
+    const V irc = IR[col.lc];
+    V d[3][5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      d[0][n] = limited_slope<V, SLOPE>(xm[n], cur[n], xp[n], H);
+      d[1][n] = limited_slope<V, SLOPE>(ym[n], cur[n], yp[n], H);
+      d[2][n] = H.zero;
+    }
+    if (SLOPE > 0) {
+      d[0][1] = momentum_bound(d[0][1], xm[0], xm[1], cur[1], xp[0], xp[1], irc, H);
+      d[1][2] = momentum_bound(d[1][2], ym[0], ym[2], cur[2], yp[0], yp[2], irc, H);
+    }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int n = 0; n < 5; ++n) d[a][n] = H.half * d[a][n];
+    V qm[3][5], qp[3][5];
+    trace_cell(cur, irc, d, qm, qp, H);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      FS[n * G::NRC + t] = qp[0][n];
+      FS[(5 + n) * G::NRC + t] = qp[1][n];
+      qmx[n] = qm[0][n];
+      qmy[n] = qm[1][n];
+    }
+  }
+  __syncthreads();
+  // (D) x flux at the right face and y flux at the top face
+  if (active) {
+    if (col.rx >= -1 && col.rx < G::CX && col.ry >= 0 && col.ry < G::CY) {
+      V qr[5], f[5];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) qr[n] = FS[n * G::NRC + t + 1];
+      riemann_dtdx<V, RIEMANN>(qmx, qr, f, H);
+#pragma unroll
+      for (int n = 0; n < 5; ++n) FXY[n * G::NRC + t] = f[n];
+    }
+    if (col.ry >= -1 && col.ry < G::CY && col.rx >= 0 && col.rx < G::CX) {
+      const int tn = t + G::RW;
+      const V ql[5] = {qmy[0], qmy[2], qmy[1], qmy[3], qmy[4]};
+      const V qr[5] = {FS[5 * G::NRC + tn], FS[7 * G::NRC + tn], FS[6 * G::NRC + tn], FS[8 * G::NRC + tn],
+                       FS[9 * G::NRC + tn]};
+      V f[5];
+      riemann_dtdx<V, RIEMANN>(ql, qr, f, H);
+      const V fy[5] = {f[0], f[2], f[1], f[3], f[4]};
+      V* FY = FXY + 5 * G::NRC;
+#pragma unroll
+      for (int n = 0; n < 5; ++n) FY[n * G::NRC + t] = fy[n];
+    }
+  }
+  __syncthreads();
+  // (E) conservative update of the tile's cells, written to both planes
+  CflAcc acc;
+  if (active && col.interior && col.in_domain_xy) {
+    const int oct = (ox0 + (col.rx >> 1)) + nxo * (oy0 + (col.ry >> 1));
+    const int c = (col.rx & 1) + 2 * (col.ry & 1);
+    const V* FX = FXY;
+    const V* FY = FXY + 5 * G::NRC;
+    if constexpr (F64) {
+      const double* o = S.uold_d + (size_t)oct * 40 + c;
+      double un[5];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        const double u0 = o[8 * n] + (FX[n * G::NRC + t - 1] - FX[n * G::NRC + t]);
+        const double up = u0 + (FY[n * G::NRC + t - G::RW] - FY[n * G::NRC + t]);
+        un[n] = up + 0.0;  // the z flux difference, an exact +0
+      }
+      double* w = S.unew_d + (size_t)oct * 40 + c;
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        w[8 * n] = un[n];
+        w[8 * n + 4] = un[n];
+      }
+      acc.add(un[0], un[1], un[2], un[3], un[4], A);
+      acc.add(un[0], un[1], un[2], un[3], un[4], A);
+    } else {
+      const float* o = S.uold_f + (size_t)oct * 32 + c;
+      float2 u2[4];
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        const float2 base = make_float2(o[8 * n], o[8 * n + 4]);
+        u2[n] = (base + (FX[n * G::NRC + t - 1] - FX[n * G::NRC + t])) +
+                (FY[n * G::NRC + t - G::RW] - FY[n * G::NRC + t]);
+      }
+      const double Eb = S.uold_d[(size_t)oct * 8 + c];
+      const double ea = (Eb + (double)(FX[4 * G::NRC + t - 1].x - FX[4 * G::NRC + t].x)) +
+                        (double)(FY[4 * G::NRC + t - G::RW].x - FY[4 * G::NRC + t].x);
+      float ua[4];
+#pragma unroll
+      for (int n = 0; n < 4; ++n) ua[n] = u2[n].x + 0.f;  // the z flux difference, an exact +0
+      const double Ea = ea + (double)0.f;
+      float* w = S.unew_f + (size_t)oct * 32 + c;
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        w[8 * n] = ua[n];
+        w[8 * n + 4] = ua[n];
+      }
+      S.unew_d[(size_t)oct * 8 + c] = Ea;
+      S.unew_d[(size_t)oct * 8 + c + 4] = Ea;
+      acc.add(ua[0], ua[1], ua[2], ua[3], Ea, A);
+      acc.add(ua[0], ua[1], ua[2], ua[3], Ea, A);
+    }
+  }
+  cfl_block_reduce<G::NWARP>(acc, A.cfl, red, out);
+}
+
+}  // namespace rh
