@@ -290,6 +290,9 @@ BatchProb make_prob(const rh_batch_problem& p, long long oct0) {
   P.tx = (p.n[0] / 2 + b.cfg.txo - 1) / b.cfg.txo;
   P.ty = (p.n[1] / 2 + b.cfg.tyo - 1) / b.cfg.tyo;
   P.tz = (p.n[2] / 2 + b.cfg.lz - 1) / b.cfg.lz;
+  // FP32-bulk 2D problems on the plane path: one work item per pair of tile rows
+  if (b.plane2d && b.precision == RH_PREC_FP32_BULK && p.ndim == 2 && p.n[2] == 2 && P.periodic[2])
+    P.ty = (P.ty + 1) / 2;
   P.dx = p.dx;
   P.gamma = p.gamma;
   P.smallr = p.smallr;

@@ -169,8 +169,10 @@ __global__ void __launch_bounds__(Geo<T, V, TXO, TYO>::NT, MINB) batch_step_kern
           const int bx = (int)(li % P.tx), by = (int)((li / P.tx) % P.ty);
           const int bz = (int)(li / ((long long)P.tx * P.ty));
           const int nzo = P.ncz >> 1;
-          rh_b_hdr = make_int4(bx * B.txo, by * B.tyo, bz * B.lz, min(B.lz, nzo - bz * B.lz));
           s_plane = B.plane2d && P.ndim == 2 && nzo == 1 && P.periodic[2];
+          // FP32-bulk plane items hold two tiles (rows 2 by and 2 by + 1) in the two lanes
+          const int ty0 = (s_plane && sizeof(T) == 4) ? 2 * by : by;
+          rh_b_hdr = make_int4(bx * B.txo, ty0 * B.tyo, bz * B.lz, min(B.lz, nzo - bz * B.lz));
           batch_level(P, dt, B.err, rh_bA);
           if constexpr (sizeof(T) == 8) {
             rh_bS64.uold_d = B.ud[parity] + P.oct0 * 40;

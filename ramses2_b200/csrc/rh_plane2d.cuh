@@ -13,6 +13,11 @@
 // without its z terms.  The CFL accumulators take each cell twice (both
 // planes), as the pencil body does.
 //
+// FP64 lanes are one cell.  FP32-bulk lanes (float2) hold two tiles of the
+// problem, TYO octs apart in y: the pencil body's two lanes are the two equal
+// planes, so pairing tiles instead halves the work per cell; each lane's
+// arithmetic is the one its cell gets in the pencil body.
+//
 // No staging: the tile's (2 TXO + 4) x (2 TYO + 4) cells are read straight from
 // the pool (a 2D tile is one layer, nothing to pipeline), converted to
 // primitives into the plane buffer, then traced, solved and updated by the
@@ -26,6 +31,36 @@ namespace rh {
 __device__ __forceinline__ int plane_oct(int v, int n, int periodic) {
   if (periodic) return ((v % n) + n) % n;
   return v < 0 ? 0 : (v >= n ? n - 1 : v);
+}
+
+// ctoprim_f32x2's arithmetic with each lane read from its own oct record and
+// its own y flip (FP32-bulk pairs two tiles of a 2D problem in the two lanes).
+__device__ __forceinline__ void ctoprim_f32_lanes(const float* sfa, const double* sda, int ca, bool fya,
+                                                  const float* sfb, const double* sdb, int cb, bool fyb, bool fx,
+                                                  const HydroK<float2>& H, double gm1, double smalle, float2* q,
+                                                  float2& ir) {
+  const float2 d = make_float2(sfa[ca], sfb[cb]);
+  float2 mx = make_float2(sfa[8 + ca], sfb[8 + cb]);
+  float2 my = make_float2(sfa[16 + ca], sfb[16 + cb]);
+  const float2 mz = make_float2(sfa[24 + ca], sfb[24 + cb]);
+  const double E0 = sda[ca], E1 = sdb[cb];
+  if (fx) mx = -mx;
+  if (fya) my.x = -my.x;
+  if (fyb) my.y = -my.y;
+  const float2 r = vmax(d, H.smallr);
+  ir = vrcp(r);
+  const float2 u = mx * ir, v = my * ir, w = mz * ir;
+  const float2 k2 = vfma(u, u, vfma(v, v, w * w));
+  double e0 = E0 - 0.5 * (double)r.x * (double)k2.x;
+  double e1 = E1 - 0.5 * (double)r.y * (double)k2.y;
+  const double m0 = smalle * (double)r.x, m1 = smalle * (double)r.y;
+  e0 = e0 > m0 ? e0 : m0;
+  e1 = e1 > m1 ? e1 : m1;
+  q[0] = r;
+  q[1] = u + H.grav[0];
+  q[2] = v + H.grav[1];
+  q[3] = w + H.grav[2];
+  q[4] = make_float2((float)(gm1 * e0), (float)(gm1 * e1));
 }
 
 template <typename T, typename V, int TXO, int TYO, int SLOPE, int RIEMANN>
@@ -54,10 +89,13 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
       double U[5];
       ctoprim_f64(S.uold_d + (size_t)oct * 40, c, mx.flip, my.flip, false, H, q, ir, U);
     } else {
-      float2 U[4];
-      double E[2];
-      ctoprim_f32x2(S.uold_f + (size_t)oct * 32, S.uold_d + (size_t)oct * 8, c, c + 4, mx.flip, my.flip, false, H,
-                    A.gm1_d, A.smalle_d, q, ir, U, E);
+      // lane .y: the same cell of the tile TYO octs further in y
+      const int gyb = gy + G::CY;
+      const CellMap myb = map_coord(gyb, A.ncy, A.periodic[1], A.btype[2], A.btype[3]);
+      const int octb = plane_oct(gx >> 1, nxo, A.periodic[0]) + nxo * plane_oct(gyb >> 1, nyo, A.periodic[1]);
+      ctoprim_f32_lanes(S.uold_f + (size_t)oct * 32, S.uold_d + (size_t)oct * 8, c, my.flip,
+                        S.uold_f + (size_t)octb * 32, S.uold_d + (size_t)octb * 8, mx.parity + 2 * myb.parity,
+                        myb.flip, mx.flip, H, A.gm1_d, A.smalle_d, q, ir);
     }
 #pragma unroll
     for (int n = 0; n < 5; ++n) Q[n * G::NLC + i] = q[n];
@@ -133,12 +171,12 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
   __syncthreads();
   // (E) conservative update of the tile's cells, written to both planes
   CflAcc acc;
-  if (active && col.interior && col.in_domain_xy) {
-    const int oct = (ox0 + (col.rx >> 1)) + nxo * (oy0 + (col.ry >> 1));
-    const int c = (col.rx & 1) + 2 * (col.ry & 1);
-    const V* FX = FXY;
-    const V* FY = FXY + 5 * G::NRC;
-    if constexpr (F64) {
+  if constexpr (F64) {
+    if (active && col.interior && col.in_domain_xy) {
+      const int oct = (ox0 + (col.rx >> 1)) + nxo * (oy0 + (col.ry >> 1));
+      const int c = (col.rx & 1) + 2 * (col.ry & 1);
+      const double* FX = FXY;
+      const double* FY = FXY + 5 * G::NRC;
       const double* o = S.uold_d + (size_t)oct * 40 + c;
       double un[5];
 #pragma unroll
@@ -155,32 +193,60 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
       }
       acc.add(un[0], un[1], un[2], un[3], un[4], A);
       acc.add(un[0], un[1], un[2], un[3], un[4], A);
-    } else {
-      const float* o = S.uold_f + (size_t)oct * 32 + c;
+    }
+  } else {
+    const int gx = 2 * ox0 + col.rx, gya = 2 * oy0 + col.ry, gyb = gya + G::CY;
+    const bool oka = active && col.interior && gx < A.ncx && gya < A.ncy;
+    const bool okb = active && col.interior && gx < A.ncx && gyb < A.ncy;
+    if (oka) {
+      const int c = (col.rx & 1) + 2 * (col.ry & 1);
+      const int octa = (gx >> 1) + nxo * (gya >> 1);
+      const int octb = okb ? (gx >> 1) + nxo * (gyb >> 1) : octa;
+      const float2* FX = FXY;
+      const float2* FY = FXY + 5 * G::NRC;
+      const float* oa = S.uold_f + (size_t)octa * 32 + c;
+      const float* ob = S.uold_f + (size_t)octb * 32 + c;
       float2 u2[4];
 #pragma unroll
       for (int n = 0; n < 4; ++n) {
-        const float2 base = make_float2(o[8 * n], o[8 * n + 4]);
+        const float2 base = make_float2(oa[8 * n], ob[8 * n]);
         u2[n] = (base + (FX[n * G::NRC + t - 1] - FX[n * G::NRC + t])) +
                 (FY[n * G::NRC + t - G::RW] - FY[n * G::NRC + t]);
       }
-      const double Eb = S.uold_d[(size_t)oct * 8 + c];
-      const double ea = (Eb + (double)(FX[4 * G::NRC + t - 1].x - FX[4 * G::NRC + t].x)) +
+      const double ea = (S.uold_d[(size_t)octa * 8 + c] + (double)(FX[4 * G::NRC + t - 1].x - FX[4 * G::NRC + t].x)) +
                         (double)(FY[4 * G::NRC + t - G::RW].x - FY[4 * G::NRC + t].x);
-      float ua[4];
-#pragma unroll
-      for (int n = 0; n < 4; ++n) ua[n] = u2[n].x + 0.f;  // the z flux difference, an exact +0
-      const double Ea = ea + (double)0.f;
-      float* w = S.unew_f + (size_t)oct * 32 + c;
+      const double eb = (S.uold_d[(size_t)octb * 8 + c] + (double)(FX[4 * G::NRC + t - 1].y - FX[4 * G::NRC + t].y)) +
+                        (double)(FY[4 * G::NRC + t - G::RW].y - FY[4 * G::NRC + t].y);
+      // the z flux differences, exact +0
+      float ua[4], ub[4];
 #pragma unroll
       for (int n = 0; n < 4; ++n) {
-        w[8 * n] = ua[n];
-        w[8 * n + 4] = ua[n];
+        ua[n] = u2[n].x + 0.f;
+        ub[n] = u2[n].y + 0.f;
       }
-      S.unew_d[(size_t)oct * 8 + c] = Ea;
-      S.unew_d[(size_t)oct * 8 + c + 4] = Ea;
+      const double Ea = ea + (double)0.f, Eb = eb + (double)0.f;
+      float* wa = S.unew_f + (size_t)octa * 32 + c;
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        wa[8 * n] = ua[n];
+        wa[8 * n + 4] = ua[n];
+      }
+      S.unew_d[(size_t)octa * 8 + c] = Ea;
+      S.unew_d[(size_t)octa * 8 + c + 4] = Ea;
       acc.add(ua[0], ua[1], ua[2], ua[3], Ea, A);
       acc.add(ua[0], ua[1], ua[2], ua[3], Ea, A);
+      if (okb) {
+        float* wb = S.unew_f + (size_t)octb * 32 + c;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+          wb[8 * n] = ub[n];
+          wb[8 * n + 4] = ub[n];
+        }
+        S.unew_d[(size_t)octb * 8 + c] = Eb;
+        S.unew_d[(size_t)octb * 8 + c + 4] = Eb;
+        acc.add(ub[0], ub[1], ub[2], ub[3], Eb, A);
+        acc.add(ub[0], ub[1], ub[2], ub[3], Eb, A);
+      }
     }
   }
   cfl_block_reduce<G::NWARP>(acc, A.cfl, red, out);

@@ -313,7 +313,8 @@ def test_batch_edge_shapes_match_oracle(n, lev, box):
 def test_batch_plane_path_equals_pencil_path(precision, slope, riemann):
     """2D problems on the plane tile body give the pencil body's result bit for
     bit (its z slopes and z flux differences are exact zeros there): several
-    boundary kinds, uneven sizes, a 3D problem in the same batch, 6 steps."""
+    boundary kinds, uneven sizes and tile-row counts (odd ones leave the last
+    FP32-bulk tile pair half empty), a 3D problem in the same batch, 6 steps."""
     cases = [((48, 32, 2), ["outflow"] * 4 + ["periodic"] * 2),
              ((16, 40, 2), ["reflexive", "outflow", "periodic", "periodic", "periodic", "periodic"]),
              ((30, 18, 2), ["reflexive"] * 4 + ["periodic"] * 2)]
@@ -339,4 +340,6 @@ def test_batch_plane_path_equals_pencil_path(precision, slope, riemann):
     for (ua, sa), (ub, sb) in zip(results[1], results[0]):
         assert np.array_equal(ua, ub)
         assert sa["t"] == sb["t"] and sa["dt"] == sb["dt"] and sa["nstep"] == sb["nstep"] == 6
-        assert sa["totals"] == sb["totals"]
+        # FP32-bulk plane items pair two tiles, so the partial sums group cells
+        # differently: the totals agree to rounding, the states bit for bit
+        assert sa["totals"] == pytest.approx(sb["totals"], rel=1e-12)
