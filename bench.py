@@ -142,19 +142,20 @@ def rel_l1(a, b):
 
 
 def time_steps(gpu, lib, steps, warmup):
-    """Per-step device time (CUDA events on the library stream); every step
-    already ends with the synchronous dt read-back of rh_cmpdt."""
+    """Per-step device time (CUDA events on the library stream) of one
+    rh_coarse_step call (courant_fine with its synchronous dt read-back,
+    set_unew, godunov_fine, set_uold)."""
     from ramses2_b200._lib import check
     import ctypes as C
 
     for _ in range(warmup):
-        gpu.step_uniform()
+        gpu.coarse_step()
     gpu.sync()
     per = []
     ms = C.c_float()
     for _ in range(steps):
         check(lib.rh_timer_start(), "rh_timer_start")
-        gpu.step_uniform()
+        gpu.coarse_step()
         check(lib.rh_timer_stop(C.byref(ms)), "rh_timer_stop")
         per.append(ms.value)
     gpu.sync()
@@ -320,7 +321,8 @@ def bench_amr(args, rank, world, dist, device):
     density/pressure gradient criterion on a developed Sedov-like blast
     (2-6 M leaf cells), HLLC, moncen, Courant 0.8, coarse steps with
     nsubcycle=1 (courant_fine of every level, then every level's Godunov
-    step).  FP64 and FP32-bulk timed over args.amr_steps steps; FP32-bulk
+    step, one rh_coarse_step call).  FP64 and FP32-bulk timed over
+    args.amr_steps steps; FP32-bulk
     relative L1 against FP64 (leaf cells) after every step of the FP64
     trajectory (same dt sequence)."""
     from ramses2_b200._abi import HydroParams
@@ -352,12 +354,15 @@ def bench_amr(args, rank, world, dist, device):
         m.uold[:] = u0
         gpu = GodunovGPU(m, P, precision=prec, device=device)
         for _ in range(2):
-            amr_coarse_step(gpu, m)
+            gpu.coarse_step()
+        # the same coarse step driven call by call from Python (a round trip per leaf call)
+        gpu.push_uold(u0)
+        per_calls = [_timed(L, lambda: amr_coarse_step(gpu, m)) for _ in range(3)]
         gpu.push_uold(u0)
         per, dts, states = [], [], []
         for _ in range(args.amr_steps):
             res = {}
-            per.append(_timed(L, lambda: res.__setitem__("dt", amr_coarse_step(gpu, m))))
+            per.append(_timed(L, lambda: res.__setitem__("dt", gpu.coarse_step())))
             dts.append(res["dt"])
             if prec == "fp64":
                 states.append(gpu.fetch_uold())
@@ -368,14 +373,15 @@ def bench_amr(args, rank, world, dist, device):
             gpu.push_uold(u0)
             errs = []
             for dt, ref in zip(*fp64_traj):
-                amr_coarse_step(gpu, m, dt)
+                gpu.coarse_step(dt)
                 errs.append(leaf_rel_l1(m, gpu.fetch_uold(), ref))
             out["fp32_bulk_vs_fp64_rel_l1_per_step"] = errs
         gpu.close()
         ms = max_over_ranks([float(np.mean(per))], dist)[0]
         out[prec] = {"value": world * leaf / (ms * 1e-3), "unit": "leaf cell-updates/s", "ms_per_coarse_step": ms,
                      "all_level_cell_updates_per_s": world * allcells / (ms * 1e-3),
-                     "ms_each_step": [round(v, 3) for v in per]}
+                     "ms_each_step": [round(v, 3) for v in per],
+                     "ms_per_coarse_step_python_leaf_calls": float(np.mean(per_calls))}
     out["fp32_bulk_over_fp64"] = out["fp64"]["ms_per_coarse_step"] / out["fp32_bulk"]["ms_per_coarse_step"]
     out["density_l1_le_1e-5"] = bool(all(e["rho"] <= 1e-5 for e in out["fp32_bulk_vs_fp64_rel_l1_per_step"]))
     out["_mesh"] = (m, P, u0)
@@ -408,8 +414,8 @@ def bench_sedov512(args, rank, world, dist, device, tuned):
         t = tuned[prec]
         gpu.set_tile(t["txo"], t["tyo"], t["lz"], t["minb"])
         for _ in range(3):
-            gpu.step_uniform()
-        ms = _timed(L, lambda: [gpu.step_uniform() for _ in range(args.sedov512_steps)]) / args.sedov512_steps
+            gpu.coarse_step()
+        ms = _timed(L, lambda: [gpu.coarse_step() for _ in range(args.sedov512_steps)]) / args.sedov512_steps
         gpu.close()
         ms = max_over_ranks([ms], dist)[0]
         v = world * ncell / (ms * 1e-3)
@@ -441,9 +447,9 @@ def bench_turbulence(args, rank, world, dist, device):
     for prec in ("fp64", "fp32_bulk"):
         m.uold[:] = u0
         gpu = GodunovGPU(m, P, precision=prec, device=device)
-        gpu.step_uniform()
+        gpu.coarse_step()
         gpu.push_uold(u0)
-        ms = _timed(L, lambda: [gpu.step_uniform() for _ in range(args.turb_steps)]) / args.turb_steps
+        ms = _timed(L, lambda: [gpu.coarse_step() for _ in range(args.turb_steps)]) / args.turb_steps
         final[prec] = gpu.fetch_uold()
         gpu.close()
         ms = max_over_ranks([ms], dist)[0]
@@ -514,7 +520,7 @@ def run_ours(args):
             check(L.rh_timer_start(), "rh_timer_start")
             for _ in range(args.steps):
                 check(L.rh_set_grid_device(dptr(host), m.ngridmax, 5, 8), "rh_set_grid_device")
-                gpu.step_uniform()
+                gpu.coarse_step()
                 check(L.rh_transfer_grid_host(dptr(host), m.ngridmax, 5, 8), "rh_transfer_grid_host")
             e2e_ms = C.c_float()
             check(L.rh_timer_stop(C.byref(e2e_ms)), "rh_timer_stop")

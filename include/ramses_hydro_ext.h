@@ -37,6 +37,17 @@ int rh_level_table(int ilevel, int* phdr, long long* poff, int* tab, long long m
  * cell | reflexive-flip bits << 3, and the father (oct, cell); returns the
  * ghost count (arrays may be null to query it), negative on error. */
 int rh_level_ghosts(int ilevel, int* gsrc_oct, unsigned char* gsrc_cf, int* gfather, long long max_ghosts);
+/* One coarse step of the whole mesh with one time step for every level
+ * (nsubcycle = 1), making the calls amr_step.f90 makes in their order:
+ * rh_cmpdt of every level, dt = min over levels of min(dx_l/smallc, cell dt)
+ * (unless *dt > 0 on entry, which is then used), rh_set_unew of every level,
+ * then from the finest level to the coarsest rh_godunov, rh_set_uold and,
+ * below the finest level, rh_upload of the level above.  dx_l = boxlen/2^l.
+ * *dt receives the time step taken; cfl (optional, 5 per level from levelmin)
+ * the courant_fine values of each level.  The same work as the separate
+ * calls, without a host round trip per call (the reference's host makes them
+ * one by one; this is for hosts that step whole meshes). */
+int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl);
 /* Where rh_set_mesh builds coarse-fine tables: 1 on the device (default),
  * 0 on the host (the reference builder the device one is tested against). */
 int rh_set_table_builder(int on_device);

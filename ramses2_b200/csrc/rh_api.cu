@@ -1037,6 +1037,53 @@ int rh_level_ghosts(int ilevel, int* gsrc_oct, unsigned char* gsrc_cf, int* gfat
   return (int)n;
 }
 
+int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
+  int rc = check_ready();
+  if (rc) return rc;
+  Context& c = ctx();
+  if (!p || !dt) {
+    set_error("rh_coarse_step: null argument");
+    return RH_EINVAL;
+  }
+  const int n3 = c.nsubgrid * c.nsubgrid * c.nsubgrid;
+  std::vector<int> lev;
+  for (int l = c.levelmin; l <= c.levelmax; ++l)
+    if (c.noct[l] > 0) lev.push_back(l);
+  auto dxl = [&](int l) { return c.boxlen / std::ldexp(1.0, l); };
+  double step_dt = *dt;
+  if (!(step_dt > 0)) {
+    step_dt = 1e300;
+    for (int l : lev) {
+      double v[5];
+      rc = rh_cmpdt(c.head[l], c.noct[l], dxl(l), p->gamma, p->smallr, p->smallc, p->courant_factor, c.gravity,
+                    &v[0], &v[1], &v[2], &v[3], &v[4]);
+      if (rc) return rc;
+      if (cfl)
+        for (int k = 0; k < 5; ++k) cfl[5 * (l - c.levelmin) + k] = v[k];
+      step_dt = std::min(step_dt, std::min(dxl(l) / p->smallc, v[4]));
+    }
+  }
+  for (int l : lev)
+    if ((rc = rh_set_unew(c.head[l], c.noct[l]))) return rc;
+  for (size_t i = lev.size(); i-- > 0;) {
+    const int l = lev[i];
+    const double dx = dxl(l);
+    rc = rh_godunov((c.head[l] - 1) / n3 + 1, c.noct[l] / n3, c.ngridmax, l, c.levelmin, c.levelmax, p->gamma,
+                    p->smallr, p->smallc * p->smallc, step_dt, dx, p->courant_factor * dx / step_dt, p->slope_type,
+                    p->riemann, c.gravity);
+    if (rc) return rc;
+    if ((rc = rh_set_uold(c.head[l], c.noct[l]))) return rc;
+    if (i + 1 < lev.size() && l + 1 <= c.levelmax && c.noct[l + 1] > 0) {
+      const int f = l + 1;
+      rc = rh_upload(c.head[f], c.noct[f], p->interpol_var == 1 ? 1 : 0, p->gamma, p->smallr,
+                     p->smallc * p->smallc);
+      if (rc) return rc;
+    }
+  }
+  *dt = step_dt;
+  return RH_OK;
+}
+
 int rh_set_table_builder(int on_device) {
   int rc = check_ready(false);
   if (rc) return rc;

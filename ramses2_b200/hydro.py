@@ -115,6 +115,12 @@ class GodunovGPU:
     def sync(self):
         check(self.L.rh_sync(), "rh_sync")
 
+    def coarse_step(self, dt=None):
+        """amr_coarse_step in one library call (rh_coarse_step): returns dt."""
+        d = C.c_double(0.0 if dt is None else float(dt))
+        check(self.L.rh_coarse_step(C.byref(self.params), C.byref(d), None), "rh_coarse_step")
+        return d.value
+
     # ---- restart / snapshot files (include/ramses_hydro_io.h) -------------------
     def file_image(self, kind):
         """Bytes of the amr / hydro_backup / hydro_output file of the current state."""

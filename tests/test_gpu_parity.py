@@ -280,6 +280,29 @@ def test_amr_steps_fp64(bc, itype, ivar, slope):
         gpu.close()
 
 
+@pytest.mark.parametrize("bc,itype,ivar", [("outflow", 1, 0), ("periodic", 2, 1)])
+def test_amr_coarse_step_native(bc, itype, ivar):
+    """rh_coarse_step (the whole level loop in one library call) against the
+    oracle's coarse steps, FP64, three steps: same dt, 1e-12 per variable."""
+    m, P = amr_case(bc, itype, ivar)
+    u0 = m.uold.copy()
+    o = oracle.OracleHydro(m, P, nthreads=NTHREADS)
+    dts, refs = [], []
+    for _ in range(3):
+        dts.append(amr_step(o, m))
+        refs.append(m.uold.copy())
+    m.uold[:] = u0
+    gpu = GodunovGPU(m, P, precision="fp64")
+    try:
+        for s in range(3):
+            dt = gpu.coarse_step()
+            assert dt == pytest.approx(dts[s], rel=1e-12)
+            err = rel_l1(gpu.fetch_uold(), refs[s])
+            assert np.all(err <= TOL_FP64), (s, err)
+    finally:
+        gpu.close()
+
+
 def test_amr_step_fp32_bulk():
     m, P = amr_case("outflow", 1, 0)
     u0 = m.uold.copy()
