@@ -12,6 +12,7 @@ whole pool is rejected.  Latency is arrival -> result on the host (for a
 burst run, where every request is due at once, start of the run -> result).
 """
 import math
+import os
 import time
 from dataclasses import dataclass, field
 
@@ -36,6 +37,7 @@ class Request:
     nsteps: int = 0
     t: float = 0.0
     result: np.ndarray = field(default=None, repr=False)
+    snapshot: str = None
     rejected: bool = False
 
     @property
@@ -130,7 +132,12 @@ class HydroServer:
     """Continuous-batching server over one device pool of ``pool_bytes``."""
 
     def __init__(self, precision="fp32_bulk", pool_bytes=8 << 30, slope_type=2, riemann="hllc", tile=None,
-                 chunk=4, keep_results=True):
+                 chunk=4, keep_results=True, snapshot_dir=None):
+        """snapshot_dir: when set, every finished request leaves an output
+        directory ``<snapshot_dir>/req<rid>/output_00001`` in the reference's
+        layout (amr and hydro files written from the device image, info.txt,
+        hydro_header.txt) before its pool range is freed."""
+        self.snapshot_dir = snapshot_dir
         self.precision = precision
         self.pool_octs = max(1, int(pool_bytes) // BYTES_PER_OCT[precision])
         self.batch = Batch(precision, slope_type=slope_type, riemann=riemann, pool_octs=self.pool_octs, tile=tile)
@@ -184,6 +191,8 @@ class HydroServer:
                     r.t = float(tt[pid])
                     if self.keep_results:
                         r.result = b.fetch(pid)
+                    if self.snapshot_dir:
+                        r.snapshot = b.write_output(pid, os.path.join(self.snapshot_dir, "req%05d" % r.rid), 1)
                     b.remove(pid)
                     r.finished = now()
                     updates += r.solved_cells * r.nsteps

@@ -56,3 +56,26 @@ def test_server_rejects_requests_larger_than_the_pool():
     finally:
         srv.close()
     assert stats["rejected"] == 3 and stats["served"] == 0
+
+
+def test_served_requests_leave_reference_layout_snapshots(tmp_path):
+    """With snapshot_dir, each finished request leaves an output directory whose
+    hydro file holds the request's final density (float32) and whose amr file
+    lists its octs; info.txt carries its step count."""
+    from ramses2_b200 import files
+
+    reqs = make_requests(4, rate_hz=1e6, seed=3, steps=(4, 8), sides_2d=(32, 32), sides_3d=(16, 16))
+    srv = HydroServer("fp64", pool_bytes=64 << 20, chunk=2, snapshot_dir=str(tmp_path))
+    try:
+        srv.run(reqs, realtime=False)
+    finally:
+        srv.close()
+    for r in reqs:
+        assert r.snapshot and sorted(__import__("os").listdir(r.snapshot)) == [
+            "amr.00001", "hydro.00001", "hydro_header.txt", "info.txt"]
+        hyd = files.parse_image(open(r.snapshot + "/hydro.00001", "rb").read(), "hydro_output")
+        amr = files.parse_image(open(r.snapshot + "/amr.00001", "rb").read(), "amr")
+        noct = r.cells // 8
+        assert hyd["noct"] == {1: noct} and amr["noct"] == {1: noct}
+        assert np.array_equal(hyd["levels"][1][:, 0, :], r.result[:, 0, :].astype(np.float32))
+        assert "nstep_coarse=%11d" % r.nsteps in open(r.snapshot + "/info.txt").read()
