@@ -84,22 +84,45 @@ int list_tiles(int prec, int amr, int* txo, int* tyo, int* minb, int max) {
 // auxiliary kernels
 // ---------------------------------------------------------------------------
 // FP32-bulk packing: [oct][5][8] double -> [oct][4][8] float + [oct][8] double
+// (one thread per cell: its 5 values)
 __global__ void pack_bulk_kernel(const double* __restrict__ src, float* __restrict__ uf, double* __restrict__ ue,
                                  long long noct) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= noct * 40) return;
-  long long oct = i / 40;
-  int r = (int)(i % 40), var = r / 8, cell = r % 8;
-  if (var < 4) uf[oct * 32 + var * 8 + cell] = (float)src[i];
-  else ue[oct * 8 + cell] = src[i];
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= noct * 8) return;
+  const long long oct = i >> 3;
+  const int cell = (int)(i & 7);
+  const double* s = src + oct * 40 + cell;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) uf[oct * 32 + v * 8 + cell] = (float)s[8 * v];
+  ue[oct * 8 + cell] = s[32];
 }
 __global__ void unpack_bulk_kernel(double* __restrict__ dst, const float* __restrict__ uf,
                                    const double* __restrict__ ue, long long noct) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= noct * 40) return;
-  long long oct = i / 40;
-  int r = (int)(i % 40), var = r / 8, cell = r % 8;
-  dst[i] = var < 4 ? (double)uf[oct * 32 + var * 8 + cell] : ue[oct * 8 + cell];
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= noct * 8) return;
+  const long long oct = i >> 3;
+  const int cell = (int)(i & 7);
+  double* d = dst + oct * 40 + cell;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) d[8 * v] = (double)uf[oct * 32 + v * 8 + cell];
+  d[32] = ue[oct * 8 + cell];
+}
+
+// FP64 staging of FP32-bulk uploads / downloads, kept between calls (a host
+// that hands its uold over every step does not pay an allocation each time).
+static int stage64(long long noct, double** out) {
+  Context& c = ctx();
+  const size_t need = sizeof(double) * 40 * (size_t)noct;
+  if (c.stage64_bytes < need) {
+    RH_CUDA(cudaStreamSynchronize(c.stream));
+    cudaFree(c.d_stage64);
+    c.d_stage64 = nullptr;
+    c.stage64_bytes = 0;
+    RH_CUDA(cudaMalloc(&c.d_stage64, need));
+    c.stage64_bytes = need;
+  }
+  *out = c.d_stage64;
+  return RH_OK;
 }
 template <typename E> __global__ void copy_kernel(E* __restrict__ dst, const E* __restrict__ src, long long n) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -248,6 +271,9 @@ static void free_state() {
   c.scratch_elems = 0;
   c.have_mesh = false;
   free_image_buffer();
+  cudaFree(c.d_stage64);
+  c.d_stage64 = nullptr;
+  c.stage64_bytes = 0;
 }
 
 // Build the pencil tables of a complete (uniform) level (on the device:
@@ -279,13 +305,11 @@ static int upload_uold(const double* uold) {
     RH_CUDA(cudaMemcpyAsync(c.ud[c.cur], uold, sizeof(double) * 40 * n, cudaMemcpyHostToDevice, c.stream));
   } else {
     double* tmp = nullptr;
-    RH_CUDA(cudaMalloc(&tmp, sizeof(double) * 40 * n));
+    int rc = stage64(n, &tmp);
+    if (rc) return rc;
     RH_CUDA(cudaMemcpyAsync(tmp, uold, sizeof(double) * 40 * n, cudaMemcpyHostToDevice, c.stream));
-    const long long tot = n * 40;
-    pack_bulk_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, c.stream>>>(tmp, c.uf[c.cur], c.ud[c.cur], n);
+    pack_bulk_kernel<<<(unsigned)((n * 8 + 255) / 256), 256, 0, c.stream>>>(tmp, c.uf[c.cur], c.ud[c.cur], n);
     RH_CUDA(cudaGetLastError());
-    RH_CUDA(cudaStreamSynchronize(c.stream));
-    cudaFree(tmp);
   }
   RH_CUDA(cudaStreamSynchronize(c.stream));
   std::fill(c.cfl_on_unew.begin(), c.cfl_on_unew.end(), 0);
@@ -625,13 +649,11 @@ int rh_transfer_grid_host(double* uold, int ngridmax, int nvar, int twotondim) {
     RH_CUDA(cudaMemcpyAsync(uold, c.ud[c.cur], sizeof(double) * 40 * n, cudaMemcpyDeviceToHost, c.stream));
   } else {
     double* tmp = nullptr;
-    RH_CUDA(cudaMalloc(&tmp, sizeof(double) * 40 * n));
-    const long long tot = n * 40;
-    unpack_bulk_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, c.stream>>>(tmp, c.uf[c.cur], c.ud[c.cur], n);
+    int rc2 = stage64(n, &tmp);
+    if (rc2) return rc2;
+    unpack_bulk_kernel<<<(unsigned)((n * 8 + 255) / 256), 256, 0, c.stream>>>(tmp, c.uf[c.cur], c.ud[c.cur], n);
     RH_CUDA(cudaGetLastError());
     RH_CUDA(cudaMemcpyAsync(uold, tmp, sizeof(double) * 40 * n, cudaMemcpyDeviceToHost, c.stream));
-    RH_CUDA(cudaStreamSynchronize(c.stream));
-    cudaFree(tmp);
   }
   RH_CUDA(cudaStreamSynchronize(c.stream));
   return RH_OK;
