@@ -44,9 +44,13 @@ int rh_level_ghosts(int ilevel, int* gsrc_oct, unsigned char* gsrc_cf, int* gfat
  * then from the finest level to the coarsest rh_godunov, rh_set_uold and,
  * below the finest level, rh_upload of the level above.  dx_l = boxlen/2^l.
  * *dt receives the time step taken; cfl (optional, 5 per level from levelmin)
- * the courant_fine values of each level.  The same work as the separate
+ * the courant_fine values of each level.  The same results as the separate
  * calls, without a host round trip per call (the reference's host makes them
- * one by one; this is for hosts that step whole meshes). */
+ * one by one; this is for hosts that step whole meshes).  When the levels
+ * hold every oct of the state, set_uold is one swap of the two state buffers
+ * after all Godunov steps and the restrictions follow, finest first: no
+ * Godunov step reads a level that an earlier set_uold or restriction of the
+ * step would have changed. */
 int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl);
 /* Where rh_set_mesh builds coarse-fine tables: 1 on the device (default),
  * 0 on the host (the reference builder the device one is tested against). */

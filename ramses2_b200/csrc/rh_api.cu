@@ -1087,6 +1087,11 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
   }
   for (int l : lev)
     if ((rc = rh_set_unew(c.head[l], c.noct[l]))) return rc;
+  // several levels that together hold every oct of the state: set_uold by one
+  // buffer swap after all Godunov steps (below); otherwise level by level
+  long long covered = 0;
+  for (int l : lev) covered += c.noct[l];
+  const bool swap_all = lev.size() > 1 && covered == c.ngridmax;
   for (size_t i = lev.size(); i-- > 0;) {
     const int l = lev[i];
     const double dx = dxl(l);
@@ -1094,12 +1099,35 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
                     p->smallr, p->smallc * p->smallc, step_dt, dx, p->courant_factor * dx / step_dt, p->slope_type,
                     p->riemann, c.gravity);
     if (rc) return rc;
-    if ((rc = rh_set_uold(c.head[l], c.noct[l]))) return rc;
-    if (i + 1 < lev.size() && l + 1 <= c.levelmax && c.noct[l + 1] > 0) {
-      const int f = l + 1;
-      rc = rh_upload(c.head[f], c.noct[f], p->interpol_var == 1 ? 1 : 0, p->gamma, p->smallr,
+    if (!swap_all && (rc = rh_set_uold(c.head[l], c.noct[l]))) return rc;
+    if (!swap_all && i + 1 < lev.size() && l + 1 <= c.levelmax && c.noct[l + 1] > 0) {
+      rc = rh_upload(c.head[l + 1], c.noct[l + 1], p->interpol_var == 1 ? 1 : 0, p->gamma, p->smallr,
                      p->smallc * p->smallc);
       if (rc) return rc;
+    }
+  }
+  if (swap_all) {
+    // Every level's unew is complete (set_unew's copy, the coarse corrections
+    // of the finer level, the level's own update), and no Godunov step of the
+    // loop above read a level whose set_uold or restriction the reference
+    // makes before it (each reads its own level and, for ghosts, the coarser
+    // one, both still old): one swap of the state buffers stands for the
+    // per-level set_uold copies, then the restrictions, finest first.
+    c.cur = 1 - c.cur;
+    for (int l : lev) {
+      c.unew_pending[l] = 0;
+      c.unew_written[l] = 0;
+      c.unew_copied[l] = 0;
+      c.cfl_on_uold[l] = c.cfl_on_unew[l];
+      c.cfl_on_unew[l] = 0;
+    }
+    for (size_t i = lev.size() - 1; i-- > 0;) {
+      const int l = lev[i];
+      if (l + 1 <= c.levelmax && c.noct[l + 1] > 0) {
+        rc = rh_upload(c.head[l + 1], c.noct[l + 1], p->interpol_var == 1 ? 1 : 0, p->gamma, p->smallr,
+                       p->smallc * p->smallc);
+        if (rc) return rc;
+      }
     }
   }
   *dt = step_dt;
