@@ -388,6 +388,7 @@ int rh_finalize(void) {
   rh_batch_free();
   free_state();
   cudaFree(c.d_err);
+  cudaFreeHost(c.h_cfl);
   cudaEventDestroy(c.ev0);
   cudaEventDestroy(c.ev1);
   cudaStreamDestroy(c.stream);
@@ -742,24 +743,21 @@ int rh_set_uold(int head_idx, int num_octs) {
   return RH_OK;
 }
 
-int rh_cmpdt(int head_idx, int num_octs, double dx, double gamma, double smallr, double smallc,
-             double courant_factor, const double* constant_gravity, double* mass, double* ekin, double* eint,
-             double* emag, double* dt) {
-  int rc = check_ready();
-  if (rc) return rc;
+}  // extern "C"
+
+// courant_fine of one level range, queued on the library stream: the five
+// reduced values land in host_out (pinned) once the stream reaches them.
+// *queued is false when there is nothing to wait for (an empty range).
+static int cmpdt_enqueue(int head_idx, int num_octs, double dx, double gamma, double smallr, double smallc,
+                         double courant_factor, const double* constant_gravity, double* host_out, bool* queued) {
   Context& c = ctx();
-  if (!mass || !ekin || !eint || !emag || !dt) {
-    set_error("rh_cmpdt: null output pointer");
-    return RH_EINVAL;
-  }
+  *queued = false;
   if (!(dx > 0) || !(gamma > 1) || !(smallc > 0) || !(courant_factor > 0)) {
     set_error("rh_cmpdt: need dx>0, gamma>1, smallc>0, courant_factor>0");
     return RH_EINVAL;
   }
   const double g[3] = {constant_gravity ? constant_gravity[0] : 0.0, constant_gravity ? constant_gravity[1] : 0.0,
                        constant_gravity ? constant_gravity[2] : 0.0};
-  *mass = *ekin = *eint = *emag = 0.0;
-  *dt = dx / smallc;  // courant_fine.f90:86
   if (num_octs == 0) return RH_OK;
   if (head_idx < 1 || num_octs < 0 || head_idx - 1 + (long long)num_octs > c.ngridmax) {
     set_error("rh_cmpdt: range outside the mesh");
@@ -769,16 +767,14 @@ int rh_cmpdt(int head_idx, int num_octs, double dx, double gamma, double smallr,
   const double key[8] = {dx, gamma, smallr, smallc, courant_factor, g[0], g[1], g[2]};
   double* lkey = l >= 0 ? &c.cfl_keys[8 * l] : nullptr;
   const bool same_key = lkey && std::equal(key, key + 8, lkey);
-  double out[5];
   if (l >= 0 && c.cfl_on_uold[l] && same_key) {
-    RH_CUDA(cudaMemcpyAsync(out, c.d_cfl + 5 * l, sizeof out, cudaMemcpyDeviceToHost, c.stream));
-    RH_CUDA(cudaStreamSynchronize(c.stream));
+    RH_CUDA(cudaMemcpyAsync(host_out, c.d_cfl + 5 * l, sizeof(double) * 5, cudaMemcpyDeviceToHost, c.stream));
   } else {
     const long long ncell = (long long)num_octs * 8;
     const int threads = 256;
     const long long nblk = (ncell + threads - 1) / threads;
     if ((size_t)nblk * 5 > c.scratch_elems) {
-      cudaFree(c.d_scratch);
+      cudaFree(c.d_scratch);  // synchronises: queued reductions are done with it
       c.d_scratch = nullptr;
       RH_CUDA(cudaMalloc(&c.d_scratch, sizeof(double) * 5 * nblk));
       c.scratch_elems = (size_t)nblk * 5;
@@ -794,16 +790,56 @@ int rh_cmpdt(int head_idx, int num_octs, double dx, double gamma, double smallr,
     double* d_out = c.d_cfl + 5 * (l >= 0 ? l : 0);
     reduce_partials_kernel<<<1, 1024, 0, c.stream>>>(c.d_scratch, nblk, 1e300, d_out);
     RH_CUDA(cudaGetLastError());
-    RH_CUDA(cudaMemcpyAsync(out, d_out, sizeof out, cudaMemcpyDeviceToHost, c.stream));
-    RH_CUDA(cudaStreamSynchronize(c.stream));
+    RH_CUDA(cudaMemcpyAsync(host_out, d_out, sizeof(double) * 5, cudaMemcpyDeviceToHost, c.stream));
     if (l >= 0) c.cfl_on_uold[l] = 0;
   }
   if (lkey) std::copy(key, key + 8, lkey);
-  *mass = out[0];
-  *ekin = out[1];
-  *eint = out[2];
+  *queued = true;
+  return RH_OK;
+}
+
+// Pinned landing area of the courant_fine values, one slot of 5 per level.
+static int cfl_host(double** out) {
+  Context& c = ctx();
+  const size_t need = 5 * (size_t)(c.levelmax + 1);
+  if (c.h_cfl_elems < need) {
+    cudaFreeHost(c.h_cfl);
+    c.h_cfl = nullptr;
+    c.h_cfl_elems = 0;
+    RH_CUDA(cudaMallocHost(&c.h_cfl, sizeof(double) * need));
+    c.h_cfl_elems = need;
+  }
+  *out = c.h_cfl;
+  return RH_OK;
+}
+
+extern "C" {
+
+int rh_cmpdt(int head_idx, int num_octs, double dx, double gamma, double smallr, double smallc,
+             double courant_factor, const double* constant_gravity, double* mass, double* ekin, double* eint,
+             double* emag, double* dt) {
+  int rc = check_ready();
+  if (rc) return rc;
+  Context& c = ctx();
+  if (!mass || !ekin || !eint || !emag || !dt) {
+    set_error("rh_cmpdt: null output pointer");
+    return RH_EINVAL;
+  }
+  *mass = *ekin = *eint = *emag = 0.0;
+  if (dx > 0 && smallc > 0) *dt = dx / smallc;  // courant_fine.f90:86
+  double* h = nullptr;
+  if ((rc = cfl_host(&h))) return rc;
+  bool queued = false;
+  if ((rc = cmpdt_enqueue(head_idx, num_octs, dx, gamma, smallr, smallc, courant_factor, constant_gravity, h,
+                          &queued)))
+    return rc;
+  if (!queued) return RH_OK;
+  RH_CUDA(cudaStreamSynchronize(c.stream));
+  *mass = h[0];
+  *ekin = h[1];
+  *eint = h[2];
   *emag = 0.0;
-  *dt = std::min(*dt, out[4]);
+  *dt = std::min(*dt, h[4]);
   return RH_OK;
 }
 
@@ -1074,15 +1110,29 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
   auto dxl = [&](int l) { return c.boxlen / std::ldexp(1.0, l); };
   double step_dt = *dt;
   if (!(step_dt > 0)) {
+    // courant_fine of every level queued back to back, one wait for all
+    double* h = nullptr;
+    if ((rc = cfl_host(&h))) return rc;
+    for (int l : lev) {
+      bool queued = false;
+      rc = cmpdt_enqueue(c.head[l], c.noct[l], dxl(l), p->gamma, p->smallr, p->smallc, p->courant_factor,
+                         c.gravity, h + 5 * l, &queued);
+      if (rc) return rc;
+    }
+    RH_CUDA(cudaStreamSynchronize(c.stream));
     step_dt = 1e300;
     for (int l : lev) {
-      double v[5];
-      rc = rh_cmpdt(c.head[l], c.noct[l], dxl(l), p->gamma, p->smallr, p->smallc, p->courant_factor, c.gravity,
-                    &v[0], &v[1], &v[2], &v[3], &v[4]);
-      if (rc) return rc;
-      if (cfl)
-        for (int k = 0; k < 5; ++k) cfl[5 * (l - c.levelmin) + k] = v[k];
-      step_dt = std::min(step_dt, std::min(dxl(l) / p->smallc, v[4]));
+      const double* v = h + 5 * l;
+      const double ldt = std::min(dxl(l) / p->smallc, v[4]);
+      if (cfl) {
+        double* o = cfl + 5 * (l - c.levelmin);
+        o[0] = v[0];
+        o[1] = v[1];
+        o[2] = v[2];
+        o[3] = 0.0;
+        o[4] = ldt;
+      }
+      step_dt = std::min(step_dt, ldt);
     }
   }
   for (int l : lev)

@@ -86,6 +86,8 @@ struct Context {
   int* d_err = nullptr;
   double* d_cfl = nullptr;        // [levelmax+1][5] reduced CFL values
   double* d_scratch = nullptr;    // standalone cmpdt partials
+  double* h_cfl = nullptr;        // pinned: courant_fine values read back, 5 per level
+  size_t h_cfl_elems = 0;
   double* d_stage64 = nullptr;    // FP64 staging of FP32-bulk uploads / downloads
   size_t stage64_bytes = 0;
   size_t scratch_elems = 0;
