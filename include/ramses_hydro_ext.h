@@ -47,7 +47,8 @@ int rh_level_ghosts(int ilevel, int* gsrc_oct, unsigned char* gsrc_cf, int* gfat
  * the courant_fine values of each level.  The same results as the separate
  * calls, without a host round trip per call (the reference's host makes them
  * one by one; this is for hosts that step whole meshes).  When the levels
- * hold every oct of the state, set_uold is one swap of the two state buffers
+ * hold every oct of the state, set_unew is one copy of the whole state and
+ * set_uold one swap of the two state buffers
  * after all Godunov steps and the restrictions follow, finest first: no
  * Godunov step reads a level that an earlier set_uold or restriction of the
  * step would have changed. */

@@ -1135,13 +1135,23 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
       step_dt = std::min(step_dt, ldt);
     }
   }
-  for (int l : lev)
-    if ((rc = rh_set_unew(c.head[l], c.noct[l]))) return rc;
-  // several levels that together hold every oct of the state: set_uold by one
-  // buffer swap after all Godunov steps (below); otherwise level by level
+  // several levels that together hold every oct of the state: set_unew as
+  // one copy of the whole state, set_uold as one buffer swap after all Godunov
+  // steps (below); otherwise level by level
   long long covered = 0;
   for (int l : lev) covered += c.noct[l];
   const bool swap_all = lev.size() > 1 && covered == c.ngridmax;
+  if (swap_all) {
+    if ((rc = copy_level(1, c.ngridmax, c.cur, 1 - c.cur))) return rc;
+    for (int l : lev) {
+      c.unew_copied[l] = 1;
+      c.unew_pending[l] = 0;
+      c.unew_written[l] = 0;
+    }
+  } else {
+    for (int l : lev)
+      if ((rc = rh_set_unew(c.head[l], c.noct[l]))) return rc;
+  }
   for (size_t i = lev.size(); i-- > 0;) {
     const int l = lev[i];
     const double dx = dxl(l);
