@@ -20,8 +20,9 @@ extern "C" {
  * accepted (rh_list_tiles). */
 int rh_set_tile(int txo, int tyo, int minb, int lz);
 /* Tile of the coarse-fine (multi-level) kernels; before rh_set_mesh, since a
- * mesh's interpolated ghost octs follow its pencils.  Default 8x4, 2 CTAs/SM,
- * 8 layers (the fastest on config 1's AMR Sedov). */
+ * mesh's interpolated ghost octs follow its pencils.  Default (the fastest on
+ * config 1's AMR Sedov): 7x7 octs, 2 CTAs/SM, 8 layers for FP32-bulk; 8x4,
+ * 2 CTAs/SM, 8 layers for FP64. */
 int rh_set_amr_tile(int txo, int tyo, int minb, int lz);
 int rh_get_tile(int* txo, int* tyo, int* minb, int* lz);
 /* Compiled tile shapes of a precision mode; returns their count. */

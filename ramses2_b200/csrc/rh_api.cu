@@ -471,6 +471,7 @@ int rh_set_amr_tile(int txo, int tyo, int minb, int lz) {
     return RH_ESTATE;
   }
   c.amr_cfg = TileCfg{txo, tyo, minb, lz};
+  c.amr_cfg_set = true;
   return RH_OK;
 }
 
@@ -478,6 +479,8 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
   int rc = check_ready(false);
   if (rc) return rc;
   Context& c = ctx();
+  // coarse-fine tile unless chosen: the fastest on config 1's AMR Sedov per precision
+  if (!c.amr_cfg_set) c.amr_cfg = c.precision == RH_PREC_FP32_BULK ? TileCfg{7, 7, 2, 8} : TileCfg{8, 4, 2, 8};
   if (!m || !uold || !m->grid || !m->head || !m->noct) {
     set_error("rh_set_mesh: null pointer");
     return RH_EINVAL;

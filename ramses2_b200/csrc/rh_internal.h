@@ -55,6 +55,7 @@ struct LevelTables {
 struct Context {
   bool inited = false;
   TileCfg amr_cfg{8, 4, 2, 8};  // tiles of multi-level meshes (coarse-fine kernels)
+  bool amr_cfg_set = false;     // amr_cfg chosen by rh_set_amr_tile (else by precision at rh_set_mesh)
   int table_builder = 1;        // coarse-fine tables: 1 on the device, 0 on the host
   int device = 0;
   int sm_count = 148;

@@ -280,11 +280,20 @@ def test_amr_steps_fp64(bc, itype, ivar, slope):
         gpu.close()
 
 
-@pytest.mark.parametrize("bc,itype,ivar", [("outflow", 1, 0), ("periodic", 2, 1)])
-def test_amr_coarse_step_native(bc, itype, ivar):
+@pytest.mark.parametrize("bc,itype,ivar,spare", [("outflow", 1, 0, 0), ("periodic", 2, 1, 0), ("outflow", 1, 0, 40)])
+def test_amr_coarse_step_native(bc, itype, ivar, spare):
     """rh_coarse_step (the whole level loop in one library call) against the
-    oracle's coarse steps, FP64, three steps: same dt, 1e-12 per variable."""
+    oracle's coarse steps, FP64, three steps: same dt, 1e-12 per variable.
+    With spare octs beyond the levels (ngridmax larger than the mesh) it
+    takes the level-by-level set_unew / set_uold path instead of the
+    whole-state copy and buffer swap."""
     m, P = amr_case(bc, itype, ivar)
+    if spare:
+        from ramses2_b200.mesh import Mesh
+        big = Mesh(m.grid, m.levelmin, m.levelmax, bc=bc, ngridmax=len(m.grid) + spare)
+        big.uold[:len(m.grid)] = m.uold
+        big.uold[len(m.grid):] = 7.0  # never part of a level: must come back unchanged
+        m = big
     u0 = m.uold.copy()
     o = oracle.OracleHydro(m, P, nthreads=NTHREADS)
     dts, refs = [], []
@@ -297,8 +306,11 @@ def test_amr_coarse_step_native(bc, itype, ivar):
         for s in range(3):
             dt = gpu.coarse_step()
             assert dt == pytest.approx(dts[s], rel=1e-12)
-            err = rel_l1(gpu.fetch_uold(), refs[s])
+            u = gpu.fetch_uold()
+            err = rel_l1(u, refs[s])
             assert np.all(err <= TOL_FP64), (s, err)
+            if spare:
+                assert np.all(u[-spare:] == 7.0)
     finally:
         gpu.close()
 
