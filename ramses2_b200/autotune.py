@@ -12,7 +12,7 @@ import os
 
 import numpy as np
 
-DEFAULT_LZ = (16, 32)
+DEFAULT_LZ = (16, 24, 32, 40)
 
 
 def tune(gpu, level, dt, lz_choices=DEFAULT_LZ, nrep=6, reps=3, log=None):
