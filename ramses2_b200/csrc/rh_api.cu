@@ -545,6 +545,13 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
                           ((long long)c.box_nx[2] << (l - 1));
     if ((long long)c.noct[l] == box) continue;
     const long long gbase = (long long)c.ngridmax + nghost;
+    // A small level gets shorter pencils so that it still fills two waves of
+    // CTAs (its pencils are few; each one marches lz layers one after the
+    // other): halve lz, down to 2, while the level's octs make fewer pencils
+    // than that.
+    TileCfg lcfg = c.amr_cfg;
+    const long long waves2 = 2LL * c.sm_count * std::max(1, lcfg.minb);
+    while (lcfg.lz > 2 && (long long)c.noct[l] / ((long long)lcfg.txo * lcfg.tyo * lcfg.lz) < waves2) lcfg.lz /= 2;
     if (c.table_builder) {
       cudaError_t e = cudaSuccess;
       if (!d_grid) {
@@ -554,11 +561,11 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
                               c.stream);
       }
       int2* gf = nullptr;
-      rc = e == cudaSuccess ? build_amr_tables_device(l, c.amr_cfg, gbase, d_grid, &gf)
+      rc = e == cudaSuccess ? build_amr_tables_device(l, lcfg, gbase, d_grid, &gf)
                             : cuda_fail(e, "oct records to the device");
       if (gf) dev_gfather.push_back({gf, gbase});
     } else {
-      rc = build_amr_tables(l, c.amr_cfg, gbase);
+      rc = build_amr_tables(l, lcfg, gbase);
     }
     if (rc) {
       drop_tables();
