@@ -581,6 +581,20 @@ def run_ours(args):
         cpu = {"value": ncell / cpu_s, "unit": "cell-updates/s", "cores": nthreads, "kind": "port",
                "sample": "one full 256^3 Sedov step (courant_fine + godunov_fine, OpenMP over oct blocks "
                          "on %d threads) of the CPU restatement of the reference path, %.2f s" % (nthreads, cpu_s)}
+        # the config-0 size (Sedov 64^3) on one thread and on all of them, a few steps each
+        from ramses2_b200.mesh import sedov3d, uniform_mesh
+
+        c0 = {}
+        for nth in (1, nthreads):
+            m0 = uniform_mesh(6, nsubgrid=1, bc="outflow")
+            sedov3d(m0, gamma=1.4, rho0=1.0, p0=1e-5, energy=1.0, radius_cells=2.0)
+            o0 = oracle.OracleHydro(m0, P, nthreads=nth)
+            o0.step_uniform()
+            t0 = time.perf_counter()
+            for _ in range(3):
+                o0.step_uniform()
+            c0["threads_%d" % nth] = 3 * int(m0.noct[6]) * 8 / (time.perf_counter() - t0)
+        cpu["sedov64_cell_updates_per_s"] = c0
         acc = {"state": "Sedov3D 256^3 after %d FP64 steps" % args.acc_steps,
                "per_step_fp32_bulk_vs_fp64_oracle_rel_l1": dict(zip(names, rel_l1(one["fp32_bulk"], ref))),
                "per_step_fp64_vs_fp64_oracle_rel_l1": dict(zip(names, rel_l1(one["fp64"], ref))),
