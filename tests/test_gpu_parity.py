@@ -315,6 +315,25 @@ def test_amr_coarse_step_native(bc, itype, ivar, spare):
         gpu.close()
 
 
+def test_amr_coarse_step_native_given_dt_fp32_bulk():
+    """rh_coarse_step with the oracle's dt passed in (no courant_fine):
+    FP32-bulk density within 1e-5 of the oracle's coarse step."""
+    m, P = amr_case("outflow", 1, 0)
+    u0 = m.uold.copy()
+    o = oracle.OracleHydro(m, P, nthreads=NTHREADS)
+    dt = amr_step(o, m)
+    ref = m.uold.copy()
+    m.uold[:] = u0
+    gpu = GodunovGPU(m, P, precision="fp32_bulk")
+    try:
+        assert gpu.coarse_step(dt) == dt
+        err = rel_l1(gpu.fetch_uold(), ref)
+    finally:
+        gpu.close()
+    assert err[0] <= TOL_FP32_RHO, err
+    assert np.all(err <= 1e-4), err
+
+
 def test_amr_step_fp32_bulk():
     m, P = amr_case("outflow", 1, 0)
     u0 = m.uold.copy()
