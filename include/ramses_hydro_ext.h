@@ -58,7 +58,9 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl);
  * 0 on the host (the reference builder the device one is tested against). */
 int rh_set_table_builder(int on_device);
 /* Device pointers of the current uold / unew buffers (FP64: *_d is
- * [oct][5][8]; FP32-bulk: *_f is [oct][4][8] float, *_d is [oct][8] energy). */
+ * [oct][5][8]; FP32-bulk: one 192-byte record per oct, 32 floats (rho, rho u,
+ * rho v, rho w of the 8 cells) then 8 doubles (E); *_f points at the first
+ * record, *_d at the first record's E, strides 48 floats / 24 doubles). */
 int rh_state_ptrs(void** uold_d, void** uold_f, void** unew_d, void** unew_f);
 /* Run nrep Godunov steps of a level with a fixed dt on the device and return
  * the average time per step from CUDA events on the library's stream. */

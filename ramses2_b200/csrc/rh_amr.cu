@@ -263,7 +263,7 @@ __global__ void prolong_kernel(const int* __restrict__ src_oct, const unsigned c
     for (int v = 0; v < 5; ++v) {
       double val;
       if (!fp32) val = ud[o * 40 + v * 8 + cell];
-      else val = v < 4 ? (double)uf[o * 32 + v * 8 + cell] : ud[o * 8 + cell];
+      else val = v < 4 ? (double)uf[o * kBulkF + v * 8 + cell] : ud[o * kBulkD + cell];
       if (v >= 1 && v <= 3 && ((cf >> (2 + v)) & 1)) val = -val;  // reflexive boundary: normal momentum
       u1[j][v] = val;
     }
@@ -309,8 +309,8 @@ __global__ void prolong_kernel(const int* __restrict__ src_oct, const unsigned c
   for (int ind = 0; ind < 8; ++ind)
     for (int v = 0; v < 5; ++v) {
       if (!fp32) ud[o * 40 + v * 8 + ind] = u2[ind][v];
-      else if (v < 4) uf[o * 32 + v * 8 + ind] = (float)u2[ind][v];
-      else ud[o * 8 + ind] = u2[ind][v];
+      else if (v < 4) uf[o * kBulkF + v * 8 + ind] = (float)u2[ind][v];
+      else ud[o * kBulkD + ind] = u2[ind][v];
     }
 }
 

@@ -83,7 +83,7 @@ int list_tiles(int prec, int amr, int* txo, int* tyo, int* minb, int max) {
 // ---------------------------------------------------------------------------
 // auxiliary kernels
 // ---------------------------------------------------------------------------
-// FP32-bulk packing: [oct][5][8] double -> [oct][4][8] float + [oct][8] double
+// FP32-bulk packing: [oct][5][8] double -> the 192-byte records of rh_bulk.h
 // (one thread per cell: its 5 values)
 __global__ void pack_bulk_kernel(const double* __restrict__ src, float* __restrict__ uf, double* __restrict__ ue,
                                  long long noct) {
@@ -93,8 +93,8 @@ __global__ void pack_bulk_kernel(const double* __restrict__ src, float* __restri
   const int cell = (int)(i & 7);
   const double* s = src + oct * 40 + cell;
 #pragma unroll
-  for (int v = 0; v < 4; ++v) uf[oct * 32 + v * 8 + cell] = (float)s[8 * v];
-  ue[oct * 8 + cell] = s[32];
+  for (int v = 0; v < 4; ++v) uf[oct * kBulkF + v * 8 + cell] = (float)s[8 * v];
+  ue[oct * kBulkD + cell] = s[32];
 }
 __global__ void unpack_bulk_kernel(double* __restrict__ dst, const float* __restrict__ uf,
                                    const double* __restrict__ ue, long long noct) {
@@ -104,8 +104,8 @@ __global__ void unpack_bulk_kernel(double* __restrict__ dst, const float* __rest
   const int cell = (int)(i & 7);
   double* d = dst + oct * 40 + cell;
 #pragma unroll
-  for (int v = 0; v < 4; ++v) d[8 * v] = (double)uf[oct * 32 + v * 8 + cell];
-  d[32] = ue[oct * 8 + cell];
+  for (int v = 0; v < 4; ++v) d[8 * v] = (double)uf[oct * kBulkF + v * 8 + cell];
+  d[32] = ue[oct * kBulkD + cell];
 }
 
 // FP64 staging of FP32-bulk uploads / downloads, kept between calls (a host
@@ -148,8 +148,8 @@ __global__ void cmpdt_kernel(const double* __restrict__ ud, const float* __restr
         const double* o = ud + oct * 40 + cell;
         r = o[0]; m1 = o[8]; m2 = o[16]; m3 = o[24]; E = o[32];
       } else {
-        const float* o = uf + oct * 32 + cell;
-        r = o[0]; m1 = o[8]; m2 = o[16]; m3 = o[24]; E = ud[oct * 8 + cell];
+        const float* o = uf + oct * kBulkF + cell;
+        r = o[0]; m1 = o[8]; m2 = o[16]; m3 = o[24]; E = ud[oct * kBulkD + cell];
       }
       m = r * vol;
       ek = E * vol;
@@ -251,8 +251,7 @@ static void free_state() {
   for (auto& t : c.levels) free_tables(t);
   c.levels.clear();
   for (int i = 0; i < 2; ++i) {
-    cudaFree(c.ud[i]);
-    cudaFree(c.uf[i]);
+    cudaFree(c.uf[i] ? (void*)c.uf[i] : (void*)c.ud[i]);  // FP32-bulk: ud is a view into uf's records
     c.ud[i] = nullptr;
     c.uf[i] = nullptr;
   }
@@ -581,8 +580,8 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
     if (c.precision == RH_PREC_FP64) {
       RH_CUDA(cudaMalloc(&c.ud[i], sizeof(double) * 40 * n));
     } else {
-      RH_CUDA(cudaMalloc(&c.uf[i], sizeof(float) * 32 * n));
-      RH_CUDA(cudaMalloc(&c.ud[i], sizeof(double) * 8 * n));
+      RH_CUDA(cudaMalloc(&c.uf[i], (size_t)kBulkBytes * n));
+      c.ud[i] = reinterpret_cast<double*>(c.uf[i]) + kBulkE;
     }
   }
   RH_CUDA(cudaMalloc(&c.d_cfl, sizeof(double) * 5 * (c.levelmax + 1)));
@@ -679,8 +678,8 @@ static int copy_level(int head_idx, int num_octs, int src, int dst) {
   if (c.precision == RH_PREC_FP64) {
     copy_kernel<double><<<blocks, threads, 0, c.stream>>>(c.ud[dst] + o0 * 40, c.ud[src] + o0 * 40, n * 40);
   } else {
-    copy_kernel<float><<<blocks, threads, 0, c.stream>>>(c.uf[dst] + o0 * 32, c.uf[src] + o0 * 32, n * 32);
-    copy_kernel<double><<<blocks, threads, 0, c.stream>>>(c.ud[dst] + o0 * 8, c.ud[src] + o0 * 8, n * 8);
+    copy_kernel<float><<<blocks, threads, 0, c.stream>>>(c.uf[dst] + o0 * kBulkF, c.uf[src] + o0 * kBulkF,
+                                                       n * kBulkF);
   }
   RH_CUDA(cudaGetLastError());
   return RH_OK;

@@ -128,8 +128,8 @@ __global__ void batch_ic_kernel(rh_batch_ic ic, BatchProb P, double* ud, float* 
   if (!fp32) {
     for (int v = 0; v < 5; ++v) ud[o * 40 + v * 8 + cell] = u[v];
   } else {
-    for (int v = 0; v < 4; ++v) uf[o * 32 + v * 8 + cell] = (float)u[v];
-    ud[o * 8 + cell] = u[4];
+    for (int v = 0; v < 4; ++v) uf[o * kBulkF + v * 8 + cell] = (float)u[v];
+    ud[o * kBulkD + cell] = u[4];
   }
 }
 
@@ -149,8 +149,8 @@ __global__ void batch_cfl_kernel(BatchProb P, const double* ud, const float* uf,
       const double* p = ud + o * 40 + cell;
       r = p[0]; m1 = p[8]; m2 = p[16]; m3 = p[24]; E = p[32];
     } else {
-      const float* p = uf + o * 32 + cell;
-      r = p[0]; m1 = p[8]; m2 = p[16]; m3 = p[24]; E = ud[o * 8 + cell];
+      const float* p = uf + o * kBulkF + cell;
+      r = p[0]; m1 = p[8]; m2 = p[16]; m3 = p[24]; E = ud[o * kBulkD + cell];
     }
     acc.add(r, m1, m2, m3, E, A);
   }
@@ -422,8 +422,8 @@ int rh_batch_init(int precision, int slope, int riemann, long long pool_octs) {
     if (precision == RH_PREC_FP64) {
       RH_CUDA(cudaMalloc(&b.ud[i], sizeof(double) * 40 * pool_octs));
     } else {
-      RH_CUDA(cudaMalloc(&b.uf[i], sizeof(float) * 32 * pool_octs));
-      RH_CUDA(cudaMalloc(&b.ud[i], sizeof(double) * 8 * pool_octs));
+      RH_CUDA(cudaMalloc(&b.uf[i], (size_t)kBulkBytes * pool_octs));
+      b.ud[i] = reinterpret_cast<double*>(b.uf[i]) + kBulkE;
     }
   }
   RH_CUDA(cudaMalloc(&b.d_prob, sizeof(BatchProb) * b.cap));
@@ -452,8 +452,7 @@ int rh_batch_free(void) {
   cudaStreamSynchronize(ctx().stream);
   if (b.graph) cudaGraphExecDestroy(b.graph);
   for (int i = 0; i < 2; ++i) {
-    cudaFree(b.ud[i]);
-    cudaFree(b.uf[i]);
+    cudaFree(b.uf[i] ? (void*)b.uf[i] : (void*)b.ud[i]);  // FP32-bulk: ud is a view into uf's records
   }
   cudaFree(b.d_prob);
   cudaFree(b.d_done);
@@ -709,14 +708,14 @@ int rh_batch_fetch(int id, double* host_uold) {
     RH_CUDA(cudaMemcpy(host_uold, b.ud[cur] + hp.oct0 * 40, sizeof(double) * 40 * hp.noct,
                        cudaMemcpyDeviceToHost));
   } else {
-    std::vector<float> f((size_t)hp.noct * 32);
-    std::vector<double> e((size_t)hp.noct * 8);
-    RH_CUDA(cudaMemcpy(f.data(), b.uf[cur] + hp.oct0 * 32, sizeof(float) * f.size(), cudaMemcpyDeviceToHost));
-    RH_CUDA(cudaMemcpy(e.data(), b.ud[cur] + hp.oct0 * 8, sizeof(double) * e.size(), cudaMemcpyDeviceToHost));
+    std::vector<float> f((size_t)hp.noct * kBulkF);  // whole records; E read through the double view
+    RH_CUDA(cudaMemcpy(f.data(), b.uf[cur] + hp.oct0 * kBulkF, (size_t)kBulkBytes * hp.noct,
+                       cudaMemcpyDeviceToHost));
+    const double* e = reinterpret_cast<const double*>(f.data()) + kBulkE;
     for (long long o = 0; o < hp.noct; ++o)
       for (int cell = 0; cell < 8; ++cell) {
-        for (int v = 0; v < 4; ++v) host_uold[o * 40 + v * 8 + cell] = (double)f[o * 32 + v * 8 + cell];
-        host_uold[o * 40 + 32 + cell] = e[o * 8 + cell];
+        for (int v = 0; v < 4; ++v) host_uold[o * 40 + v * 8 + cell] = (double)f[o * kBulkF + v * 8 + cell];
+        host_uold[o * 40 + 32 + cell] = e[o * kBulkD + cell];
       }
   }
   return RH_OK;
@@ -737,8 +736,8 @@ int rh_batch_file_image(int id, int kind, void* host_buf, long long cap, long lo
   RH_CUDA(cudaMemcpy(&cur, b.d_cur + id, sizeof(int), cudaMemcpyDeviceToHost));
   ImageSrc s;
   s.bulk = b.precision == RH_PREC_FP32_BULK;
-  s.ud = b.ud[cur] + hp.oct0 * (s.bulk ? 8 : 40);
-  s.uf = s.bulk ? b.uf[cur] + hp.oct0 * 32 : nullptr;
+  s.ud = b.ud[cur] + hp.oct0 * (s.bulk ? kBulkD : 40);
+  s.uf = s.bulk ? b.uf[cur] + hp.oct0 * kBulkF : nullptr;
   s.levelmin = s.levelmax = 1;
   s.oct0.push_back(0);
   s.noct.push_back(hp.noct);

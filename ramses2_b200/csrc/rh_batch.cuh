@@ -34,8 +34,8 @@ struct BatchArgs {
   const int* done;
   const double* dt;
   double* partial;          // [nwork][5]
-  double* ud[2];            // FP64 pool [oct][5][8], or FP32-bulk energy [oct][8]
-  float* uf[2];             // FP32-bulk pool [oct][4][8]
+  double* ud[2];            // FP64 pool [oct][5][8], or the FP32-bulk records' E view
+  float* uf[2];             // FP32-bulk pool: 192-byte records (rh_bulk.h)
   int* err;
   int plane2d;              // 2D problems take the plane tile body (else the pencil body)
 };
@@ -181,10 +181,10 @@ __global__ void __launch_bounds__(Geo<T, V, TXO, TYO>::NT, MINB) batch_step_kern
             rh_bS64.unew_f = nullptr;
             batch_hydro<double>(P, dt, rh_bH64);
           } else {
-            rh_bS32.uold_d = B.ud[parity] + P.oct0 * 8;
-            rh_bS32.unew_d = B.ud[1 - parity] + P.oct0 * 8;
-            rh_bS32.uold_f = B.uf[parity] + P.oct0 * 32;
-            rh_bS32.unew_f = B.uf[1 - parity] + P.oct0 * 32;
+            rh_bS32.uold_d = B.ud[parity] + P.oct0 * kBulkD;
+            rh_bS32.unew_d = B.ud[1 - parity] + P.oct0 * kBulkD;
+            rh_bS32.uold_f = B.uf[parity] + P.oct0 * kBulkF;
+            rh_bS32.unew_f = B.uf[1 - parity] + P.oct0 * kBulkF;
             batch_hydro<float2>(P, dt, rh_bH32);
           }
         }

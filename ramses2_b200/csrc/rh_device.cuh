@@ -10,6 +10,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "rh_bulk.h"
+
 namespace rh {
 
 // ---------------------------------------------------------------------------

@@ -93,10 +93,10 @@ __device__ __forceinline__ void load(const double* ud, const float* uf, int fp32
 #pragma unroll
     for (int v = 0; v < 5; ++v) u[v] = s[8 * v];
   } else {
-    const float* s = uf + oct * 32 + cell;
+    const float* s = uf + oct * kBulkF + cell;
 #pragma unroll
     for (int v = 0; v < 4; ++v) u[v] = (double)s[8 * v];
-    u[4] = ud[oct * 8 + cell];
+    u[4] = ud[oct * kBulkD + cell];
   }
 }
 

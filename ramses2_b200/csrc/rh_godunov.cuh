@@ -45,10 +45,10 @@ template <> struct Store<double> {  // plain FP64: reference layout [oct][5][8]
   static constexpr int kSlotD = 42;  // doubles per staged oct (40 + pad)
   static constexpr uint32_t kBytes = 320;
 };
-template <> struct Store<float> {  // FP32-bulk: [oct][4][8] float + [oct][8] double (E)
-  static constexpr int kSlotF = 36;  // 32 + pad
-  static constexpr int kSlotD = 10;  // 8 + pad
-  static constexpr uint32_t kBytes = 128 + 64;
+template <> struct Store<float> {  // FP32-bulk: one 192-byte record per oct (rh_bulk.h)
+  static constexpr int kSlotF = 52;  // 48 + pad (floats per staged record)
+  static constexpr int kSlotD = 0;
+  static constexpr uint32_t kBytes = kBulkBytes;
 };
 
 // T: storage element of the bulk variables; V: lane type of the arithmetic.
@@ -160,15 +160,15 @@ __device__ __forceinline__ void coarse_add_f32(const LevelArgs& A, float* unew_f
                                                const float* f, float sign) {
   const int2 fa = A.ghost_father[ghost_ent - A.ghost_base];
   if (fa.x < 0) return;
-  float* o = unew_f + (size_t)fa.x * 32 + fa.y;
+  float* o = unew_f + (size_t)fa.x * kBulkF + fa.y;
 #pragma unroll
   for (int n = 0; n < 4; ++n) atomicAdd(o + 8 * n, sign * (f[n] * 0.125f));
-  atomicAdd(unew_e + (size_t)fa.x * 8 + fa.y, (double)sign * ((double)f[4] * 0.125));
+  atomicAdd(unew_e + (size_t)fa.x * kBulkD + fa.y, (double)sign * ((double)f[4] * 0.125));
 }
 
 template <typename T> struct StateArgs {
-  const double* uold_d;  // FP64 [oct][5][8]  or FP32-bulk energy [oct][8]
-  const float* uold_f;   // FP32-bulk [oct][4][8]
+  const double* uold_d;  // FP64 [oct][5][8]  or the FP32-bulk records' E view (rh_bulk.h)
+  const float* uold_f;   // FP32-bulk records
   double* unew_d;
   float* unew_f;
 };
@@ -363,8 +363,8 @@ template <typename T, class G, bool DENSE = false> struct Stager {
         if (sizeof(T) == 8) {
           bulk_g2s(stageD + ((size_t)st * G::NSLOT + t) * Store<T>::kSlotD, src_d + (size_t)oct * 40, 320, &bar[st]);
         } else {
-          bulk_g2s(stageF + ((size_t)st * G::NSLOT + t) * Store<T>::kSlotF, src_f + (size_t)oct * 32, 128, &bar[st]);
-          bulk_g2s(stageD + ((size_t)st * G::NSLOT + t) * Store<T>::kSlotD, src_d + (size_t)oct * 8, 64, &bar[st]);
+          bulk_g2s(stageF + ((size_t)st * G::NSLOT + t) * Store<T>::kSlotF, src_f + (size_t)oct * kBulkF, kBulkBytes,
+                   &bar[st]);
         }
       } else {
         mbar_arrive_expect_tx(&bar[st], 0);
@@ -377,6 +377,8 @@ template <typename T, class G, bool DENSE = false> struct Stager {
     bounded_mbar_wait(&bar[st], par, s_abort, err, kWaitBound);
   }
   __device__ __forceinline__ const double* slot_d(int row, int slot) const {
+    if (sizeof(T) == 4)  // FP32-bulk: the staged record's E, after its 32 floats
+      return reinterpret_cast<const double*>(slot_f(row, slot) + 32);
     return stageD + ((size_t)((rb() + row) % G::NSTAGE) * G::NSLOT + slot) * Store<T>::kSlotD;
   }
   __device__ __forceinline__ const float* slot_f(int row, int slot) const {

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "ramses_hydro.h"
+#include "rh_bulk.h"
 
 namespace rh {
 
@@ -74,7 +75,7 @@ struct Context {
   std::vector<rh_oct> grid;
   std::vector<int> head, noct;
   std::vector<LevelTables> levels;
-  // device state: FP64 -> ud[2] = [oct][5][8]; FP32-bulk -> uf[2] = [oct][4][8], ud[2] = [oct][8]
+  // device state: FP64 -> ud[2] = [oct][5][8]; FP32-bulk -> uf[2] = records of rh_bulk.h, ud[2] their E view
   int cur = 0;
   double* ud[2] = {nullptr, nullptr};
   float* uf[2] = {nullptr, nullptr};
@@ -117,8 +118,8 @@ int build_complete_tables_device(int l, const TileCfg& cfg, LevelTables& T);
 
 // restart / snapshot file images (rh_io.cu)
 struct ImageSrc {
-  const double* ud = nullptr;  // FP64: [oct][5][8]; FP32-bulk: E [oct][8]
-  const float* uf = nullptr;   // FP32-bulk: [oct][4][8]
+  const double* ud = nullptr;  // FP64: [oct][5][8]; FP32-bulk: the records' E view (rh_bulk.h)
+  const float* uf = nullptr;   // FP32-bulk: the records' float view
   int bulk = 0;
   int levelmin = 1, levelmax = 1;
   std::vector<long long> oct0, noct;  // per level from levelmin: first oct (0-based) and count

@@ -56,12 +56,12 @@ __global__ void prim_image_kernel(const double* __restrict__ ud, const float* __
   const int cell = (int)(i & 7);
   double d, mx, my, mz, e;
   if (bulk) {
-    const float* f = uf + o * 32 + cell;
+    const float* f = uf + o * kBulkF + cell;
     d = f[0];
     mx = f[8];
     my = f[16];
     mz = f[24];
-    e = ud[o * 8 + cell];
+    e = ud[o * kBulkD + cell];
   } else {
     const double* u = ud + o * 40 + cell;
     d = u[0];
@@ -91,11 +91,11 @@ __global__ void state_image_kernel(const double* __restrict__ ue, const float* _
   if (i >= noct * 8) return;
   const long long o = i >> 3;
   const int cell = (int)(i & 7);
-  const float* f = uf + o * 32 + cell;
+  const float* f = uf + o * kBulkF + cell;
   double v[5];
 #pragma unroll
   for (int k = 0; k < 4; ++k) v[k] = (double)f[8 * k];
-  v[4] = ue[o * 8 + cell];
+  v[4] = ue[o * kBulkD + cell];
   uint32_t* w = dst + o * 80 + 2 * cell;
 #pragma unroll
   for (int k = 0; k < 5; ++k) {
@@ -119,10 +119,10 @@ __global__ void state_restore_kernel(const uint32_t* __restrict__ src, long long
   for (int k = 0; k < 5; ++k)
     v[k] = __longlong_as_double((long long)((unsigned long long)w[16 * k] |
                                             ((unsigned long long)w[16 * k + 1] << 32)));
-  float* f = uf + o * 32 + cell;
+  float* f = uf + o * kBulkF + cell;
 #pragma unroll
   for (int k = 0; k < 4; ++k) f[8 * k] = (float)v[k];
-  ue[o * 8 + cell] = v[4];
+  ue[o * kBulkD + cell] = v[4];
 }
 
 bool valid_kind(int kind) {
@@ -228,13 +228,13 @@ int build_image(int kind, const ImageSrc& s, double gamma, const void** dimage, 
       if (n == 0) continue;
       uint32_t* dst = (uint32_t*)(img + off);
       if (kind == RH_FILE_HYDRO_OUTPUT) {
-        const double* ud = s.bulk ? s.ud + o0 * 8 : s.ud + o0 * 40;
-        const float* uf = s.bulk ? s.uf + o0 * 32 : nullptr;
+        const double* ud = s.bulk ? s.ud + o0 * kBulkD : s.ud + o0 * 40;
+        const float* uf = s.bulk ? s.uf + o0 * kBulkF : nullptr;
         prim_image_kernel<<<blocks_for(n * 8, threads), threads, 0, c.stream>>>(ud, uf, s.bulk, n, gamma - 1.0,
                                                                                dst);
       } else if (s.bulk) {
-        state_image_kernel<<<blocks_for(n * 8, threads), threads, 0, c.stream>>>(s.ud + o0 * 8, s.uf + o0 * 32, n,
-                                                                               dst);
+        state_image_kernel<<<blocks_for(n * 8, threads), threads, 0, c.stream>>>(s.ud + o0 * kBulkD,
+                                                                               s.uf + o0 * kBulkF, n, dst);
       } else {
         RH_CUDA(cudaMemcpyAsync(dst, s.ud + o0 * 40, (size_t)n * 320, cudaMemcpyDeviceToDevice, c.stream));
       }
@@ -373,7 +373,7 @@ int rh_restore_hydro(const void* image, long long nbytes) {
       const long long n = noct[li], o0 = c.head[c.levelmin + li] - 1;
       if (n) {
         state_restore_kernel<<<blocks_for(n * 8, threads), threads, 0, c.stream>>>(
-            (const uint32_t*)((const char*)g_image + off), n, c.uf[c.cur] + o0 * 32, c.ud[c.cur] + o0 * 8);
+            (const uint32_t*)((const char*)g_image + off), n, c.uf[c.cur] + o0 * kBulkF, c.ud[c.cur] + o0 * kBulkD);
         RH_CUDA(cudaGetLastError());
       }
       off += n * 320;

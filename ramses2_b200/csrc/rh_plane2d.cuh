@@ -93,8 +93,8 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
       const int gyb = gy + G::CY;
       const CellMap myb = map_coord(gyb, A.ncy, A.periodic[1], A.btype[2], A.btype[3]);
       const int octb = plane_oct(gx >> 1, nxo, A.periodic[0]) + nxo * plane_oct(gyb >> 1, nyo, A.periodic[1]);
-      ctoprim_f32_lanes(S.uold_f + (size_t)oct * 32, S.uold_d + (size_t)oct * 8, c, my.flip,
-                        S.uold_f + (size_t)octb * 32, S.uold_d + (size_t)octb * 8, mx.parity + 2 * myb.parity,
+      ctoprim_f32_lanes(S.uold_f + (size_t)oct * kBulkF, S.uold_d + (size_t)oct * kBulkD, c, my.flip,
+                        S.uold_f + (size_t)octb * kBulkF, S.uold_d + (size_t)octb * kBulkD, mx.parity + 2 * myb.parity,
                         myb.flip, mx.flip, H, A.gm1_d, A.smalle_d, q, ir);
     }
 #pragma unroll
@@ -204,8 +204,8 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
       const int octb = okb ? (gx >> 1) + nxo * (gyb >> 1) : octa;
       const float2* FX = FXY;
       const float2* FY = FXY + 5 * G::NRC;
-      const float* oa = S.uold_f + (size_t)octa * 32 + c;
-      const float* ob = S.uold_f + (size_t)octb * 32 + c;
+      const float* oa = S.uold_f + (size_t)octa * kBulkF + c;
+      const float* ob = S.uold_f + (size_t)octb * kBulkF + c;
       float2 u2[4];
 #pragma unroll
       for (int n = 0; n < 4; ++n) {
@@ -213,9 +213,9 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
         u2[n] = (base + (FX[n * G::NRC + t - 1] - FX[n * G::NRC + t])) +
                 (FY[n * G::NRC + t - G::RW] - FY[n * G::NRC + t]);
       }
-      const double ea = (S.uold_d[(size_t)octa * 8 + c] + (double)(FX[4 * G::NRC + t - 1].x - FX[4 * G::NRC + t].x)) +
+      const double ea = (S.uold_d[(size_t)octa * kBulkD + c] + (double)(FX[4 * G::NRC + t - 1].x - FX[4 * G::NRC + t].x)) +
                         (double)(FY[4 * G::NRC + t - G::RW].x - FY[4 * G::NRC + t].x);
-      const double eb = (S.uold_d[(size_t)octb * 8 + c] + (double)(FX[4 * G::NRC + t - 1].y - FX[4 * G::NRC + t].y)) +
+      const double eb = (S.uold_d[(size_t)octb * kBulkD + c] + (double)(FX[4 * G::NRC + t - 1].y - FX[4 * G::NRC + t].y)) +
                         (double)(FY[4 * G::NRC + t - G::RW].y - FY[4 * G::NRC + t].y);
       // the z flux differences, exact +0
       float ua[4], ub[4];
@@ -225,25 +225,25 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
         ub[n] = u2[n].y + 0.f;
       }
       const double Ea = ea + (double)0.f, Eb = eb + (double)0.f;
-      float* wa = S.unew_f + (size_t)octa * 32 + c;
+      float* wa = S.unew_f + (size_t)octa * kBulkF + c;
 #pragma unroll
       for (int n = 0; n < 4; ++n) {
         wa[8 * n] = ua[n];
         wa[8 * n + 4] = ua[n];
       }
-      S.unew_d[(size_t)octa * 8 + c] = Ea;
-      S.unew_d[(size_t)octa * 8 + c + 4] = Ea;
+      S.unew_d[(size_t)octa * kBulkD + c] = Ea;
+      S.unew_d[(size_t)octa * kBulkD + c + 4] = Ea;
       acc.add(ua[0], ua[1], ua[2], ua[3], Ea, A);
       acc.add(ua[0], ua[1], ua[2], ua[3], Ea, A);
       if (okb) {
-        float* wb = S.unew_f + (size_t)octb * 32 + c;
+        float* wb = S.unew_f + (size_t)octb * kBulkF + c;
 #pragma unroll
         for (int n = 0; n < 4; ++n) {
           wb[8 * n] = ub[n];
           wb[8 * n + 4] = ub[n];
         }
-        S.unew_d[(size_t)octb * 8 + c] = Eb;
-        S.unew_d[(size_t)octb * 8 + c + 4] = Eb;
+        S.unew_d[(size_t)octb * kBulkD + c] = Eb;
+        S.unew_d[(size_t)octb * kBulkD + c + 4] = Eb;
         acc.add(ub[0], ub[1], ub[2], ub[3], Eb, A);
         acc.add(ub[0], ub[1], ub[2], ub[3], Eb, A);
       }

@@ -69,8 +69,8 @@ __device__ __forceinline__ double ekin_of(double r, double m1, double m2, double
   return e;
 }
 
-// One fine oct per thread.  FP64: ud = [oct][5][8].  FP32-bulk: uf = [oct][4][8]
-// (rho, momentum) and ud = [oct][8] (E); averages taken in FP64.
+// One fine oct per thread.  FP64: ud = [oct][5][8].  FP32-bulk: the records
+// of rh_bulk.h through their float (uf) and E (ud) views; averages in FP64.
 __global__ void upload_kernel(double* __restrict__ ud, float* __restrict__ uf, int fp32,
                               const int2* __restrict__ father, long long o0, long long n, int internal_energy,
                               double smallr) {
@@ -87,13 +87,13 @@ __global__ void upload_kernel(double* __restrict__ ud, float* __restrict__ uf, i
 #pragma unroll
       for (int c = 0; c < 8; ++c) u[v][c] = s[v * 8 + c];
   } else {
-    const float* s = uf + o * 32;
+    const float* s = uf + o * kBulkF;
 #pragma unroll
     for (int v = 0; v < 4; ++v)
 #pragma unroll
       for (int c = 0; c < 8; ++c) u[v][c] = (double)s[v * 8 + c];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) u[4][c] = ud[o * 8 + c];
+    for (int c = 0; c < 8; ++c) u[4][c] = ud[o * kBulkD + c];
   }
   double a[5];
 #pragma unroll
@@ -118,10 +118,10 @@ __global__ void upload_kernel(double* __restrict__ ud, float* __restrict__ uf, i
 #pragma unroll
     for (int v = 0; v < 5; ++v) d[v * 8] = a[v];
   } else {
-    float* d = uf + p * 32 + fa.y;
+    float* d = uf + p * kBulkF + fa.y;
 #pragma unroll
     for (int v = 0; v < 4; ++v) d[v * 8] = (float)a[v];
-    ud[p * 8 + fa.y] = a[4];
+    ud[p * kBulkD + fa.y] = a[4];
   }
 }
 
