@@ -209,6 +209,36 @@ struct CflAcc {
     if (C.ndim > 2) ctot += fabs(w) + c;
     cmax = ctot > cmax ? ctot : cmax;
   }
+  // The same quantities for an FP32-bulk cell (density and momenta held in
+  // FP32, E in FP64), in fewer FP64 operations: the three sums stay unscaled
+  // until scale_bulk multiplies them by the cell volume once, the kinetic
+  // energy is (m1^2 + m2^2 + m3^2) / (2 rho) (the squares of FP32 momenta
+  // are exact in FP64) and ctot = (|m1| + |m2| + |m3|) / rho + ndim c.
+  __device__ __forceinline__ void add_bulk(float rf, float m1f, float m2f, float m3f, double E,
+                                           const LevelArgs& A) {
+    const CflConst& C = A.cfl;
+    const double r = rf, m1 = m1f, m2 = m2f, m3 = m3f;
+    mass += r;
+    ekin += E;
+    const double rm = r > C.smallr ? r : C.smallr;
+    const double irm = vrcp(rm);
+    const double e = fma(-0.5 * fma(m1, m1, fma(m2, m2, m3 * m3)), irm, E);
+    eint += e;
+    double p = C.gm1 * e;
+    const double pf = rm * C.smallp;
+    p = p > pf ? p : pf;
+    const double c = vsqrt(C.gamma * p * irm);
+    double a = fabs(m1);
+    if (C.ndim > 1) a += fabs(m2);
+    if (C.ndim > 2) a += fabs(m3);
+    const double ctot = fma(a, irm, (double)C.ndim * c);
+    cmax = ctot > cmax ? ctot : cmax;
+  }
+  __device__ __forceinline__ void scale_bulk(double vol) {
+    mass *= vol;
+    ekin *= vol;
+    eint *= vol;
+  }
   // smallest cell dt of the accumulated cells (1e300 when there were none)
   __device__ __forceinline__ double dt(const CflConst& C) const {
     if (!(cmax > 0.0)) return 1e300;

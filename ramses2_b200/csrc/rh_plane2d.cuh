@@ -233,8 +233,8 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
       }
       S.unew_d[(size_t)octa * kBulkD + c] = Ea;
       S.unew_d[(size_t)octa * kBulkD + c + 4] = Ea;
-      acc.add(ua[0], ua[1], ua[2], ua[3], Ea, A);
-      acc.add(ua[0], ua[1], ua[2], ua[3], Ea, A);
+      acc.add_bulk(ua[0], ua[1], ua[2], ua[3], Ea, A);
+      acc.add_bulk(ua[0], ua[1], ua[2], ua[3], Ea, A);
       if (okb) {
         float* wb = S.unew_f + (size_t)octb * kBulkF + c;
 #pragma unroll
@@ -244,11 +244,12 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
         }
         S.unew_d[(size_t)octb * kBulkD + c] = Eb;
         S.unew_d[(size_t)octb * kBulkD + c + 4] = Eb;
-        acc.add(ub[0], ub[1], ub[2], ub[3], Eb, A);
-        acc.add(ub[0], ub[1], ub[2], ub[3], Eb, A);
+        acc.add_bulk(ub[0], ub[1], ub[2], ub[3], Eb, A);
+        acc.add_bulk(ub[0], ub[1], ub[2], ub[3], Eb, A);
       }
     }
   }
+  if constexpr (!F64) acc.scale_bulk(A.vol);
   cfl_block_reduce<G::NWARP>(acc, A.cfl, red, out);
 }
 
