@@ -231,6 +231,40 @@ def test_one_step_fp32_bulk(case):
     assert np.all(err <= 1e-4), err
 
 
+def test_fp32_bulk_courant_fine_on_its_state():
+    """courant_fine of an FP32-bulk state: the values fused into the Godunov
+    kernel (FP64 sums and dt over the new FP32 density and momenta and FP64
+    energy) and the standalone reduction of the same state re-uploaded both
+    match exact sums of the cell terms and the oracle's courant_fine on that
+    state (the fetched values are exact: FP32 widened, FP64 energy)."""
+    import math
+
+    m = uniform_mesh(5, nsubgrid=1, bc="outflow")
+    g = blast_state(m, 11, 1.4)
+    P = HydroParams.make(gamma=g, courant_factor=0.8, slope_type=2, riemann="hllc")
+    gpu = GodunovGPU(m, P, precision="fp32_bulk")
+    try:
+        gpu.step_uniform()
+        fused = gpu.courant_fine(5)
+        u = gpu.fetch_uold()
+        gpu.push_uold(u)
+        alone = gpu.courant_fine(5)
+    finally:
+        gpu.close()
+    mo = uniform_mesh(5, nsubgrid=1, bc="outflow")
+    mo.uold[:] = u
+    o = oracle.OracleHydro(mo, P).courant_fine(5)
+    vol = m.dx(5) ** 3
+    lu = u[m.level_slice(5)]
+    mass = math.fsum((lu[:, 0, :] * vol).ravel())
+    etot = math.fsum((lu[:, 4, :] * vol).ravel())
+    for c in (fused, alone):
+        assert c[0] == pytest.approx(mass, rel=1e-13)
+        assert c[1] == pytest.approx(etot, rel=1e-13)
+        assert c[2] == pytest.approx(o[2], rel=1e-10)
+        assert c[4] == pytest.approx(o[4], rel=1e-13)
+
+
 # ---------------------------------------------------------------------------
 # Coarse-fine (AMR) levels
 # ---------------------------------------------------------------------------
