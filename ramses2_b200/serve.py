@@ -20,7 +20,8 @@ import numpy as np
 
 from .batch import Batch, ic_blast, ic_split, problem, random_state
 
-BYTES_PER_OCT = {"fp64": 2 * 320, "fp32_bulk": 2 * (128 + 64)}
+# device bytes per oct: uold + unew (FP64: 320-byte records; FP32-bulk: 192-byte records)
+BYTES_PER_OCT = {"fp64": 2 * 320, "fp32_bulk": 2 * 192}
 
 
 @dataclass
