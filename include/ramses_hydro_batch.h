@@ -70,7 +70,8 @@ int rh_batch_capacity(void);
 /* Copy a problem's current state to the host, reference layout, row-major octs. */
 int rh_batch_fetch(int id, double* host_uold);
 /* Tile of the batch kernel (one of the compiled shapes rh_batch_list_tiles
- * returns; lz = oct layers per pencil). */
+ * returns; lz = oct layers per pencil).  rh_batch_init starts from 7x7 octs,
+ * 2 CTAs per SM, 32 layers (FP32-bulk) or 8x4 / 2 / 32 (FP64). */
 int rh_batch_set_tile(int txo, int tyo, int minb, int lz);
 /* Compiled batch-kernel shapes of a precision: writes up to max entries,
  * returns how many exist. */

@@ -290,9 +290,12 @@ BatchProb make_prob(const rh_batch_problem& p, long long oct0) {
   P.tx = (p.n[0] / 2 + b.cfg.txo - 1) / b.cfg.txo;
   P.ty = (p.n[1] / 2 + b.cfg.tyo - 1) / b.cfg.tyo;
   P.tz = (p.n[2] / 2 + b.cfg.lz - 1) / b.cfg.lz;
-  // FP32-bulk 2D problems on the plane path: one work item per pair of tile rows
-  if (b.plane2d && b.precision == RH_PREC_FP32_BULK && p.ndim == 2 && p.n[2] == 2 && P.periodic[2])
-    P.ty = (P.ty + 1) / 2;
+  // 2D problems on the plane path: one work item per kPlaneGroup tile bodies
+  // along y (FP32-bulk tile bodies take two tile rows, one per lane)
+  if (b.plane2d && p.ndim == 2 && p.n[2] == 2 && P.periodic[2]) {
+    const int bodies = b.precision == RH_PREC_FP32_BULK ? (P.ty + 1) / 2 : P.ty;
+    P.ty = (bodies + kPlaneGroup - 1) / kPlaneGroup;
+  }
   P.dx = p.dx;
   P.gamma = p.gamma;
   P.smallr = p.smallr;
@@ -417,6 +420,9 @@ int rh_batch_init(int precision, int slope, int riemann, long long pool_octs) {
   b.slope = slope;
   b.riemann = riemann;
   b.pool_octs = pool_octs;
+  // default tile per precision: the fastest of the autotuner's sweep on the
+  // uneven 3D ensemble and on mixed 2D/3D serving
+  b.cfg = precision == RH_PREC_FP32_BULK ? TileCfg{7, 7, 2, 32} : TileCfg{8, 4, 2, 32};
   b.cap = 4096;
   for (int i = 0; i < 2; ++i) {
     if (precision == RH_PREC_FP64) {

@@ -9,6 +9,10 @@ namespace rh {
 
 constexpr int kBatchMaxLz = 64;      // most oct layers of one batch pencil
 constexpr int kBatchMaxSlots = 100;  // most oct columns (tile + halo) of one batch pencil
+// Tile bodies per work item of a 2D problem on the plane path: a plane tile is
+// one layer, so the item set-up (work counter, slot search, problem constants)
+// is shared by this many tiles along y.
+constexpr int kPlaneGroup = 4;
 
 // Static description of one problem in the device pool.
 struct BatchProb {
@@ -130,12 +134,24 @@ __device__ __noinline__ void batch_pencil(int rbase) {
 // One XY tile of a 2D problem (rh_plane2d.cuh), out of line like batch_pencil.
 template <typename T, int TXO, int TYO, int SLOPE, int RIEMANN>
 __device__ __noinline__ void batch_plane() {
-  const int4 hdr = rh_b_hdr;
-  if constexpr (sizeof(T) == 8) {
-    plane2d_body<T, double, TXO, TYO, SLOPE, RIEMANN>(rh_bA, rh_bS64, rh_bH64, hdr, rh_b_out);
-  } else {
-    plane2d_body<T, float2, TXO, TYO, SLOPE, RIEMANN>(rh_bA, rh_bS32, rh_bH32, hdr, rh_b_out);
+  using V = typename std::conditional<sizeof(T) == 8, double, float2>::type;
+  using G = Geo<T, V, TXO, TYO>;
+  constexpr int rows = sizeof(T) == 8 ? 1 : 2;  // tile rows per tile body (FP32-bulk: two, one per lane)
+  const int4 h0 = rh_b_hdr;
+  const int nyo = rh_bA.ncy >> 1;
+  CflAcc acc;
+  for (int g = 0; g < kPlaneGroup; ++g) {
+    const int4 hdr = make_int4(h0.x, h0.y + g * rows * TYO, h0.z, h0.w);
+    if (hdr.y >= nyo) break;
+    if (g) __syncthreads();
+    if constexpr (sizeof(T) == 8) {
+      plane2d_body<T, double, TXO, TYO, SLOPE, RIEMANN>(rh_bA, rh_bS64, rh_bH64, hdr, acc);
+    } else {
+      plane2d_body<T, float2, TXO, TYO, SLOPE, RIEMANN>(rh_bA, rh_bS32, rh_bH32, hdr, acc);
+    }
   }
+  if constexpr (sizeof(T) == 4) acc.scale_bulk(rh_bA.vol);
+  cfl_block_reduce<G::NWARP>(acc, rh_bA.cfl, reinterpret_cast<double*>(rh_smem + G::oRed), rh_b_out);
 }
 
 template <typename T, typename V, int TXO, int TYO, int MINB, int SLOPE, int RIEMANN>
@@ -170,8 +186,9 @@ __global__ void __launch_bounds__(Geo<T, V, TXO, TYO>::NT, MINB) batch_step_kern
           const int bz = (int)(li / ((long long)P.tx * P.ty));
           const int nzo = P.ncz >> 1;
           s_plane = B.plane2d && P.ndim == 2 && nzo == 1 && P.periodic[2];
-          // FP32-bulk plane items hold two tiles (rows 2 by and 2 by + 1) in the two lanes
-          const int ty0 = (s_plane && sizeof(T) == 4) ? 2 * by : by;
+          // a plane item is kPlaneGroup tile bodies along y; FP32-bulk tile
+          // bodies hold two tile rows, one in each lane
+          const int ty0 = s_plane ? by * kPlaneGroup * (sizeof(T) == 4 ? 2 : 1) : by;
           rh_b_hdr = make_int4(bx * B.txo, ty0 * B.tyo, bz * B.lz, min(B.lz, nzo - bz * B.lz));
           batch_level(P, dt, B.err, rh_bA);
           if constexpr (sizeof(T) == 8) {

@@ -65,14 +65,13 @@ __device__ __forceinline__ void ctoprim_f32_lanes(const float* sfa, const double
 
 template <typename T, typename V, int TXO, int TYO, int SLOPE, int RIEMANN>
 __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs<T>& S, const HydroK<V>& H,
-                                             const int4 hdr, double* out) {
+                                             const int4 hdr, CflAcc& acc) {
   constexpr bool F64 = sizeof(T) == 8;
   using G = Geo<T, V, TXO, TYO>;
   V* Q = reinterpret_cast<V*>(rh_smem + G::oQ);  // [5][NLC] primitives, then [NLC] 1/rho
   V* IR = Q + 5 * G::NLC;
   V* FS = reinterpret_cast<V*>(rh_smem + G::oFS);   // [10][NRC]: qp_x(5), qp_y(5)
   V* FXY = reinterpret_cast<V*>(rh_smem + G::oFX);  // [2][5][NRC]: x then y fluxes
-  double* red = reinterpret_cast<double*>(rh_smem + G::oRed);
   const int t = threadIdx.x;
   const int ox0 = hdr.x, oy0 = hdr.y;
   const int nxo = A.ncx >> 1, nyo = A.ncy >> 1;
@@ -170,7 +169,6 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
   }
   __syncthreads();
   // (E) conservative update of the tile's cells, written to both planes
-  CflAcc acc;
   if constexpr (F64) {
     if (active && col.interior && col.in_domain_xy) {
       const int oct = (ox0 + (col.rx >> 1)) + nxo * (oy0 + (col.ry >> 1));
@@ -249,8 +247,6 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
       }
     }
   }
-  if constexpr (!F64) acc.scale_bulk(A.vol);
-  cfl_block_reduce<G::NWARP>(acc, A.cfl, red, out);
 }
 
 }  // namespace rh
