@@ -314,10 +314,13 @@ def test_batch_plane_path_equals_pencil_path(precision, slope, riemann):
     """2D problems on the plane tile body give the pencil body's result bit for
     bit (its z slopes and z flux differences are exact zeros there): several
     boundary kinds, uneven sizes and tile-row counts (odd ones leave the last
-    FP32-bulk tile pair half empty), a 3D problem in the same batch, 6 steps."""
+    FP32-bulk tile pair half empty), a tall problem whose work items hold
+    several tile bodies along y (the last item only part of a group), a 3D
+    problem in the same batch, 6 steps."""
     cases = [((48, 32, 2), ["outflow"] * 4 + ["periodic"] * 2),
              ((16, 40, 2), ["reflexive", "outflow", "periodic", "periodic", "periodic", "periodic"]),
-             ((30, 18, 2), ["reflexive"] * 4 + ["periodic"] * 2)]
+             ((30, 18, 2), ["reflexive"] * 4 + ["periodic"] * 2),
+             ((24, 232, 2), ["outflow"] * 2 + ["periodic"] * 4)]
     results = {}
     for plane in (1, 0):
         b = Batch(precision, slope_type=slope, riemann=riemann, pool_octs=1 << 14)
