@@ -141,20 +141,17 @@ __device__ __noinline__ void batch_pencil(int rbase) {
 
 // One XY tile of a 2D problem (rh_plane2d.cuh), out of line like batch_pencil.
 template <typename T, int TXO, int TYO, int SLOPE, int RIEMANN>
-__device__ __noinline__ void batch_plane(int g) {
-  using V = typename std::conditional<sizeof(T) == 8, double, float2>::type;
-  using G = Geo<T, V, TXO, TYO>;
+__device__ __noinline__ void batch_plane(int g, CflAcc* acc) {
   constexpr int rows = sizeof(T) == 8 ? 1 : 2;  // tile rows per tile body (FP32-bulk: two, one per lane)
   const int4 h0 = rh_b_hdr;
   const int4 hdr = make_int4(h0.x, h0.y + g * rows * TYO, h0.z, h0.w);
-  CflAcc acc;
+  CflAcc a = *acc;
   if constexpr (sizeof(T) == 8) {
-    plane2d_body<T, double, TXO, TYO, SLOPE, RIEMANN>(rh_bA, rh_bS64, rh_bH64, hdr, acc);
+    plane2d_body<T, double, TXO, TYO, SLOPE, RIEMANN>(rh_bA, rh_bS64, rh_bH64, hdr, a);
   } else {
-    plane2d_body<T, float2, TXO, TYO, SLOPE, RIEMANN>(rh_bA, rh_bS32, rh_bH32, hdr, acc);
-    acc.scale_bulk(rh_bA.vol);
+    plane2d_body<T, float2, TXO, TYO, SLOPE, RIEMANN>(rh_bA, rh_bS32, rh_bH32, hdr, a);
   }
-  cfl_block_reduce<G::NWARP>(acc, rh_bA.cfl, reinterpret_cast<double*>(rh_smem + G::oRed), rh_b_out, g > 0);
+  *acc = a;
 }
 
 template <typename T, typename V, int TXO, int TYO, int MINB, int SLOPE, int RIEMANN>
@@ -219,10 +216,13 @@ __global__ void __launch_bounds__(Geo<T, V, TXO, TYO>::NT, MINB) batch_step_kern
     if (s_skip) continue;
     if (s_plane) {
       const int rows = sizeof(T) == 8 ? 1 : 2;
+      CflAcc acc;
       for (int g = 0; g < kPlaneGroup && rh_b_hdr.y + g * rows * TYO < (rh_bA.ncy >> 1); ++g) {
         if (g) __syncthreads();
-        batch_plane<T, TXO, TYO, SLOPE, RIEMANN>(g);
+        batch_plane<T, TXO, TYO, SLOPE, RIEMANN>(g, &acc);
       }
+      if constexpr (sizeof(T) == 4) acc.scale_bulk(rh_bA.vol);
+      cfl_block_reduce<G::NWARP>(acc, rh_bA.cfl, reinterpret_cast<double*>(rh_smem + G::oRed), rh_b_out);
       continue;
     }
     {

@@ -256,8 +256,7 @@ struct CflAcc {
 
 // Deterministic block reduction of the CFL accumulators into the pencil partial.
 template <int NWARP>
-__device__ __forceinline__ void cfl_block_reduce(const CflAcc& a, const CflConst& C, double* red, double* out,
-                                                 bool combine = false) {
+__device__ __forceinline__ void cfl_block_reduce(const CflAcc& a, const CflConst& C, double* red, double* out) {
   double v[4] = {a.mass, a.ekin, a.eint, a.dt(C)};
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
@@ -277,10 +276,6 @@ __device__ __forceinline__ void cfl_block_reduce(const CflAcc& a, const CflConst
     for (int w = 0; w < NWARP; ++w) {
       s0 += red[w * 4 + 0]; s1 += red[w * 4 + 1]; s2 += red[w * 4 + 2];
       d = red[w * 4 + 3] < d ? red[w * 4 + 3] : d;
-    }
-    if (combine) {  // fold into the partial already written by this work item
-      s0 += out[0]; s1 += out[1]; s2 += out[2];
-      d = out[4] < d ? out[4] : d;
     }
     out[0] = s0; out[1] = s1; out[2] = s2; out[3] = 0.0; out[4] = d;
   }
