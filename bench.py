@@ -135,6 +135,14 @@ def make_problem():
     return m, P
 
 
+def bench_config(world, ncell):
+    """The workload description both arms print (same keys, same values)."""
+    return {"workload": WORKLOAD, "grid": "256^3 uniform (levelmin=levelmax=8)", "problem": "Sedov3D",
+            "riemann": "hllc", "slope": "moncen", "courant": 0.8, "boundary": "outflow",
+            "cells": ncell, "parallelism": "replicas" if world > 1 else "single-gpu",
+            "l2": "state (>=805 MB) larger than L2 (126 MB); no flush needed"}
+
+
 def rel_l1(a, b):
     num = np.abs(a - b).sum(axis=(0, 2))
     den = np.abs(b).sum(axis=(0, 2))
@@ -191,21 +199,47 @@ def bench_batch(args, rank, world, dist):
         best, _ = b.tune()
         for pid in list(b.problems):
             b.remove(pid)
+        pids = []
         for p, ic in ens:
             p.max_steps = args.batch_steps
-            b.add(p, ic)
+            pids.append(b.add(p, ic))
+        sample = batch_sample(ens)
+        init = {i: b.fetch_dense(pids[i]) for i in sample}
         if dist is not None:
             dist.barrier()
         with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
             ms = b.bench(args.batch_steps)
         done, nstep, _ = b.poll()
         ok = bool(done[:len(ens)].all() and (nstep[:len(ens)] == args.batch_steps).all())
+        out.setdefault("_oracle_sample", {})[prec] = [
+            {"problem": ens[i][0], "init": init[i], "final": b.fetch_dense(pids[i]), "nstep": int(nstep[pids[i]]),
+             "t": float(b.status(pids[i])["t"]), "label": "ensemble[%d] side %d" % (i, ens[i][0].n[0])}
+            for i in sample]
         b.close()
         ms = max_over_ranks([ms], dist)[0]
         out[prec] = {"value": out["cells"] / (ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms,
                      "tile": best, "all_problems_finished": ok, "clocks": clk.summary()}
     out["fp32_bulk_over_fp64"] = out["fp64"]["ms_per_step"] / out["fp32_bulk"]["ms_per_step"]
     return out
+
+
+def batch_sample(ens, per_side=((16, 2), (32, 2), (48, 1))):
+    """Indices of the ensemble problems whose results are checked against
+    the oracle: the first few of the smallest sides (the oracle must solve
+    each one for all its steps on the host)."""
+    out = []
+    for side, k in per_side:
+        out += [i for i, (p, _) in enumerate(ens) if p.n[0] == side][:k]
+    return out
+
+
+def serve_sample(reqs, k2=2, k3=2):
+    """Request ids checked against the oracle: the k2 2D and k3 3D requests of
+    least work (cells x target steps)."""
+    work = lambda r: r.solved_cells * r.target_steps  # noqa: E731
+    two = sorted((r for r in reqs if int(r.prob.ndim) == 2), key=work)[:k2]
+    three = sorted((r for r in reqs if int(r.prob.ndim) == 3), key=work)[:k3]
+    return [r.rid for r in two + three]
 
 
 def bench_serve(args, rank, world, dist):
@@ -224,9 +258,24 @@ def bench_serve(args, rank, world, dist):
         srv = HydroServer(prec, pool_bytes=16 << 30, chunk=4, keep_results=False)
         srv.run(make_requests(4, rate_hz=1e6, seed=1, steps=(4, 8)), realtime=False)  # warm-up
         reqs = make_requests(args.serve_requests, rate_hz=args.serve_rate, seed=20261203 + rank)
+        keep = serve_sample(reqs)
+        srv.keep_results = set(keep)
         if dist is not None:
             dist.barrier()
         st = srv.run(reqs, realtime=True)
+        srv.keep_results = False
+        samples = []
+        for r in reqs:
+            if r.rid in keep and r.result is not None:
+                pid = srv.batch.add(r.prob, r.ic)  # the request's initial state, as the device builds it
+                init = srv.batch.fetch_dense(pid)
+                srv.batch.remove(pid)
+                from ramses2_b200.batch import octs_to_dense
+
+                samples.append({"problem": r.prob, "init": init, "final": octs_to_dense(r.result, tuple(r.prob.n)),
+                                "nstep": r.nsteps, "t": r.t,
+                                "label": "request %d %s %s" % (r.rid, r.kind, "x".join(str(v) for v in r.prob.n))})
+        out.setdefault("_oracle_sample", {})[prec] = samples
         # capacity: the same requests all due at once (closed loop)
         burst = make_requests(args.serve_requests, rate_hz=args.serve_rate, seed=20261203 + rank)
         if dist is not None:
@@ -317,14 +366,15 @@ def leaf_rel_l1(m, a, b):
 
 
 def bench_amr(args, rank, world, dist, device):
-    """Config-1 style AMR Sedov: levels 7-10 refined by hydro_refine's 0.1
+    """Config 1: AMR Sedov on levels 7-10 refined by hydro_refine's 0.1
     density/pressure gradient criterion on a developed Sedov-like blast
-    (2-6 M leaf cells), HLLC, moncen, Courant 0.8, coarse steps with
-    nsubcycle=1 (courant_fine of every level, then every level's Godunov
-    step, one rh_coarse_step call).  FP64 and FP32-bulk timed over
-    args.amr_steps steps; FP32-bulk
-    relative L1 against FP64 (leaf cells) after every step of the FP64
-    trajectory (same dt sequence)."""
+    (2-6 M leaf cells), HLLC, moncen, Courant 0.8, args.amr_steps coarse
+    steps with nsubcycle=1 (courant_fine of every level, then every level's
+    Godunov step, one rh_coarse_step call), FP64 and FP32-bulk, each timed
+    step by step.  Along the FP64 run the state before every
+    args.amr_check_every-th step is kept (the oracle takes one coarse step
+    from each later, on the host); the FP32-bulk run is repeated along the
+    FP64 dt sequence and compared with those states (cumulative error)."""
     from ramses2_b200._abi import HydroParams
     from ramses2_b200._lib import lib
     from ramses2_b200.hydro import GodunovGPU, amr_coarse_step
@@ -340,7 +390,10 @@ def bench_amr(args, rank, world, dist, device):
     allcells = int(m.noct_total) * 8
     out = {"workload": "AMR Sedov, levels 7-10, hydro_refine err_grad_d = err_grad_p = 0.1 on a developed blast",
            "leaf_cells": leaf, "cells_all_levels": allcells,
-           "octs_per_level": {str(l): int(m.noct[l]) for l in range(7, 11)}, "steps": args.amr_steps}
+           "octs_per_level": {str(l): int(m.noct[l]) for l in range(7, 11)}, "steps": args.amr_steps,
+           "check_every": args.amr_check_every}
+    checks = set(range(0, args.amr_steps, max(1, args.amr_check_every)))
+    keep_states = rank == 0 and not args.no_cpu
     # coarse-fine table build (rh_set_mesh wall time, FP64 state upload
     # included): best of three after one untimed warm-up build
     build_s = {"host": [], "device": []}
@@ -360,23 +413,26 @@ def bench_amr(args, rank, world, dist, device):
         gpu.push_uold(u0)
         per_calls = [_timed(L, lambda: amr_coarse_step(gpu, m)) for _ in range(3)]
         gpu.push_uold(u0)
-        per, dts, states = [], [], []
-        for _ in range(args.amr_steps):
+        per, dts, states = [], [], {}
+        for s in range(args.amr_steps):
+            if prec == "fp64" and s in checks:
+                states[s] = gpu.fetch_uold()  # untimed: the state before step s+1
             res = {}
             per.append(_timed(L, lambda: res.__setitem__("dt", gpu.coarse_step())))
             dts.append(res["dt"])
-            if prec == "fp64":
-                states.append(gpu.fetch_uold())
         if prec == "fp64":
             fp64_traj = (dts, states)
         else:
-            # accuracy along the FP64 trajectory: same dt sequence, untimed
+            # cumulative accuracy along the FP64 trajectory: same dt sequence, untimed
             gpu.push_uold(u0)
             errs = []
-            for dt, ref in zip(*fp64_traj):
+            for s, dt in enumerate(fp64_traj[0]):
+                if s in checks and s > 0:
+                    e = leaf_rel_l1(m, gpu.fetch_uold(), fp64_traj[1][s])
+                    e["after_steps"] = s
+                    errs.append(e)
                 gpu.coarse_step(dt)
-                errs.append(leaf_rel_l1(m, gpu.fetch_uold(), ref))
-            out["fp32_bulk_vs_fp64_rel_l1_per_step"] = errs
+            out["fp32_bulk_vs_fp64_trajectory_rel_l1"] = errs
         gpu.close()
         ms = max_over_ranks([float(np.mean(per))], dist)[0]
         out[prec] = {"value": world * leaf / (ms * 1e-3), "unit": "leaf cell-updates/s", "ms_per_coarse_step": ms,
@@ -384,9 +440,58 @@ def bench_amr(args, rank, world, dist, device):
                      "ms_each_step": [round(v, 3) for v in per],
                      "ms_per_coarse_step_python_leaf_calls": float(np.mean(per_calls))}
     out["fp32_bulk_over_fp64"] = out["fp64"]["ms_per_coarse_step"] / out["fp32_bulk"]["ms_per_coarse_step"]
-    out["density_l1_le_1e-5"] = bool(all(e["rho"] <= 1e-5 for e in out["fp32_bulk_vs_fp64_rel_l1_per_step"]))
-    out["_mesh"] = (m, P, u0)
+    out["_mesh"] = (m, P, u0, fp64_traj if keep_states else None)
     return out
+
+
+def amr_oracle_checks(m, P, traj, oracle, nthreads, device):
+    """Per-step accuracy along the FP64 AMR run: from each kept state S_k (the
+    state before step k+1) the oracle takes one coarse step with the dt the
+    GPU took there, and so do the FP64 and FP32-bulk GPU paths (a fresh
+    context each, pushed S_k); leaf-cell relative L1 of each against the
+    oracle, and the oracle's own courant_fine dt against the GPU's."""
+    from ramses2_b200.hydro import GodunovGPU, amr_coarse_step
+
+    if traj is None:
+        return []
+    dts, states = traj
+    lev = [l for l in range(m.levelmin, m.levelmax + 1) if m.noct[l]]
+    out = []
+    for k in sorted(states):
+        s_k = states[k]
+        m.uold[:] = s_k
+        o = oracle.OracleHydro(m, P, nthreads=nthreads)
+        dt_or = min(min(m.dx(l) / P.smallc, o.courant_fine(l)[4]) for l in lev)
+        amr_coarse_step(o, m, dts[k])
+        ref = m.uold.copy()
+        c = {"step": k + 1, "dt_gpu": dts[k], "dt_oracle_rel_diff": abs(dt_or / dts[k] - 1.0)}
+        for prec in ("fp64", "fp32_bulk"):
+            m.uold[:] = s_k
+            gpu = GodunovGPU(m, P, precision=prec, device=device)
+            gpu.coarse_step(dts[k])
+            c[prec] = leaf_rel_l1(m, gpu.fetch_uold(), ref)
+            gpu.close()
+        out.append(c)
+    m.uold[:] = states[min(states)]
+    return out
+
+
+def sample_vs_oracle(s, oracle, nthreads):
+    """One batch problem or served request solved by the oracle from the
+    state the device started it from, to the same stopping rule: relative L1
+    per conserved variable of the device's final state, and both step counts."""
+    from ramses2_b200._abi import HydroParams
+
+    p = s["problem"]
+    P = HydroParams.make(gamma=p.gamma, smallr=p.smallr, smallc=p.smallc, courant_factor=p.courant_factor,
+                         slope_type=2, riemann="hllc")
+    ref, t, ns = oracle.solve_box(s["init"], p.dx, P, bc=[int(v) for v in p.bound_type], ndim=int(p.ndim),
+                                  t_end=p.t_end, max_steps=p.max_steps, nthreads=nthreads)
+    num = np.abs(s["final"] - ref).sum(axis=(1, 2, 3))
+    den = np.abs(ref).sum(axis=(1, 2, 3))
+    l1 = num / np.where(den > 0, den, 1.0)
+    return {"problem": s["label"], "rel_l1": dict(zip(["rho", "mx", "my", "mz", "E"], l1.tolist())),
+            "steps": s["nstep"], "oracle_steps": ns, "t_rel_diff": abs(s["t"] / t - 1.0) if t else None}
 
 
 PUBLISHED_512 = {"fp64": 4456e6, "fp32_bulk": 10093e6}  # reference B200, hydro double/single NSUBGRID=4
@@ -606,18 +711,17 @@ def run_ours(args):
         from ramses2_b200.hydro import amr_coarse_step
 
         if amr is not None:
-            ma, Pa, ua = amr.pop("_mesh")
-            ma.uold[:] = ua
-            oa = oracle.OracleHydro(ma, Pa, nthreads=nthreads)
-            dta = amr_coarse_step(oa, ma)
-            refa = ma.uold.copy()
-            amr["one_step_vs_oracle_rel_l1"] = {}
-            for prec in ("fp64", "fp32_bulk"):
-                ma.uold[:] = ua
-                gpu = GodunovGPU(ma, Pa, precision=prec, device=device)
-                amr_coarse_step(gpu, ma, dta)
-                amr["one_step_vs_oracle_rel_l1"][prec] = leaf_rel_l1(ma, gpu.fetch_uold(), refa)
-                gpu.close()
+            ma, Pa, ua, traj = amr.pop("_mesh")
+            amr["per_step_vs_oracle"] = amr_oracle_checks(ma, Pa, traj, oracle, nthreads, device)
+            amr["fp64_per_step_le_1e-12"] = bool(all(
+                max(c["fp64"][k] for k in names) <= 1e-12 for c in amr["per_step_vs_oracle"]))
+            amr["fp32_bulk_density_le_1e-5"] = bool(
+                all(c["fp32_bulk"]["rho"] <= 1e-5 for c in amr["per_step_vs_oracle"]) and
+                all(e["rho"] <= 1e-5 for e in amr["fp32_bulk_vs_fp64_trajectory_rel_l1"]))
+        for leg in (batch, serve):
+            if leg is not None and "_oracle_sample" in leg:
+                leg["results_vs_oracle"] = {p: [sample_vs_oracle(s, oracle, nthreads) for s in v]
+                                            for p, v in leg.pop("_oracle_sample").items()}
         if turb is not None:
             mt, Pt, st = turb.pop("_state")
             mt.uold[:] = st
@@ -635,6 +739,9 @@ def run_ours(args):
         amr.pop("_mesh", None)
     if turb is not None:
         turb.pop("_state", None)
+    for leg in (batch, serve):
+        if leg is not None:
+            leg.pop("_oracle_sample", None)
     peak, peak_kind = measured_peaks()
     prec = "fp32_bulk"
     ms = results[prec]["ms_per_step"]
@@ -655,10 +762,7 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "fp32+fp64(E,p,dt,sums)",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": "256^3 uniform (levelmin=levelmax=8)", "problem": "Sedov3D",
-                   "riemann": "hllc", "slope": "moncen", "courant": 0.8, "boundary": "outflow",
-                   "cells": ncell, "parallelism": "replicas" if world > 1 else "single-gpu",
-                   "l2": "state (>=805 MB) larger than L2 (126 MB); no flush needed"},
+        "config": bench_config(world, ncell),
         "fp64": {"value": world * ncell / (results["fp64"]["ms_per_step"] * 1e-3),
                  "ms_per_step": results["fp64"]["ms_per_step"],
                  "kernel_ms": kernel_ms["fp64"],
@@ -725,8 +829,7 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": "256^3 uniform (levelmin=levelmax=8)", "problem": "Sedov3D",
-                   "riemann": "hllc", "slope": "moncen", "courant": 0.8, "boundary": "outflow", "cells": ncell},
+        "config": bench_config(world, ncell),
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": nthreads, "kind": "port",
                          "sample": "full 256^3 Sedov steps of the CPU restatement of the reference path "
                                    "(Fortran reference not compilable in this image)"},
@@ -744,7 +847,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / accuracy leg")
     ap.add_argument("--acc-steps", type=int, default=100, help="steps before the accuracy comparison")
     ap.add_argument("--sedov512-steps", type=int, default=5, help="periodic Sedov 512^3 steps (0: skip)")
-    ap.add_argument("--amr-steps", type=int, default=10, help="AMR Sedov coarse steps (0: skip)")
+    ap.add_argument("--amr-steps", type=int, default=200, help="AMR Sedov coarse steps (0: skip)")
+    ap.add_argument("--amr-check-every", type=int, default=10,
+                    help="oracle check of the AMR run before every n-th coarse step")
     ap.add_argument("--turb-steps", type=int, default=100, help="turbulence 256^3 steps (0: skip)")
     ap.add_argument("--batch-problems", type=int, default=1024, help="batched ensemble size (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=50)
@@ -753,8 +858,6 @@ def main():
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
-        args.steps = min(args.steps, 3)
-        args.warmup = 1
         run_reference(args)
     else:
         run_ours(args)

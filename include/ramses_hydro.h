@@ -2,7 +2,7 @@
  * ramses_hydro.h — C ABI of the B200-native RAMSES II Godunov hydro step.
  *
  * This is the drop-in boundary for RAMSES II's hydro leaf calls.  The Fortran
- * host reaches it through iso_c_binding; every entry
+ * host reaches it through an iso_c_binding interface module; every entry
  * point takes plain pointers, sizes and scalars, returns 0 on success and a
  * nonzero RH_E* code on failure (message in rh_last_error()).  The reference
  * aborts on errors (GPU_Error_Check, gpu/gpu_utils.cuf:59-79; error stop in

@@ -95,7 +95,13 @@ int rh_timer_stop(float* ms);
  * clearing, and every call reuses the same array: calls that overlap on the
  * GPU (different streams, or host threads sharing a device) race.  The first
  * call on a device looks up the array's device address (cudaGetSymbolAddress)
- * and caches it; make that first call before any stream capture.
+ * and caches it; make that first call before any stream capture.  Every later
+ * call made outside capture looks the address up again; a call on a stream
+ * being captured uses the cached one, so after a device reset make one call
+ * outside capture before capturing again.  Under CUDA's lazy module loading
+ * (the default since CUDA 12.2) the array's 2.6 MB are reserved on the device
+ * when that first call runs: a host whose memory manager reserves the whole
+ * device budget makes the first call before that reservation.
  * Asynchronous: read d_out after synchronising the stream. */
 int rh_cmpdt_noalloc(const double* d_uold, int num_octs, const unsigned char* d_refined, double dx,
                      double gamma, double smallr, double smallc, double courant_factor,

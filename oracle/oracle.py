@@ -27,6 +27,18 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
+def reference_root():
+    """The reference checkout the CPU checks may read (environment variable
+    REF_ROOT, else the default of oracle/Makefile), or None when it is absent
+    (as on a machine that only runs the tests)."""
+    root = os.environ.get("REF_ROOT")
+    if not root:
+        r = subprocess.run(["make", "-s", "--no-print-directory", "-C", HERE, "print-ref-root"],
+                           capture_output=True, text=True)
+        root = r.stdout.strip() if r.returncode == 0 else ""
+    return root if root and os.path.isdir(root) else None
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -40,6 +52,9 @@ def lib():
                                         P(HydroParams), P(C.c_double)]
         L.rh_oracle_cmpdt.argtypes = [P(C.c_double), P(C.c_double), C.c_double, P(HydroParams), C.c_int]
         L.rh_oracle_cmpdt.restype = C.c_double
+        L.rh_oracle_cmpdt_octs.argtypes = [P(C.c_double), C.c_longlong, P(C.c_double), C.c_double, P(HydroParams),
+                                           C.c_int, C.c_int]
+        L.rh_oracle_cmpdt_octs.restype = C.c_double
         L.rh_oracle_interpol_hydro.argtypes = [P(C.c_double), P(C.c_double), C.c_int, C.c_int, C.c_double]
         L.rh_oracle_godunov_fine.argtypes = [P(MeshDesc), P(HydroParams), C.c_int, C.c_double,
                                              P(C.c_double), P(C.c_double), C.c_int]
@@ -80,6 +95,41 @@ def cmpdt(uu, dx, params, grav=(0.0, 0.0, 0.0), ndim=3):
     uu = np.ascontiguousarray(uu, np.float64)
     g = np.ascontiguousarray(grav, np.float64)
     return lib().rh_oracle_cmpdt(dptr(uu), dptr(g), dx, C.byref(params), ndim)
+
+
+def cmpdt_octs(uold, dx, params, ndim=3, grav=(0.0, 0.0, 0.0), nthreads=1):
+    """Smallest cell dt (cmpdt) over a (noct, 5, 8) state, in ndim directions."""
+    u = np.ascontiguousarray(uold, np.float64)
+    g = np.ascontiguousarray(grav, np.float64)
+    return lib().rh_oracle_cmpdt_octs(dptr(u), len(u), dptr(g), dx, C.byref(params), ndim, nthreads)
+
+
+def solve_box(dense, dx, params, bc="outflow", ndim=3, t_end=0.0, max_steps=0, nthreads=1):
+    """One single-level problem of the batch runtime solved by the oracle to
+    its stopping rule, in the order the batch follows (the reference's coarse
+    step, amr/amr_step.f90, with newdt_fine's dt = min(dx/smallc, courant
+    dt) cut to land on t_end): courant_fine dt of the state (ndim
+    directions; a 2D problem is a two-cell-deep periodic z slab), set_unew,
+    godunov_fine, set_uold, until t >= t_end (relative 1e-12) or max_steps
+    steps.  dense: (5, nz, ny, nx) conserved state of even extents.
+    Returns (final dense state, t, steps)."""
+    from ramses2_b200.mesh import uniform_mesh
+
+    nz, ny, nx = dense.shape[1:]
+    m = uniform_mesh(1, nsubgrid=1, boxlen=2.0 * dx, bc=bc, box_nx=(nx // 2, ny // 2, nz // 2))
+    assert m.dx(1) == dx
+    m.from_dense(dense, 1)
+    o = OracleHydro(m, params, nthreads=nthreads)
+    t, ns = 0.0, 0
+    while True:
+        dt = min(dx / params.smallc, cmpdt_octs(m.uold, dx, params, ndim=ndim, nthreads=nthreads))
+        if t_end > 0.0 and t + dt > t_end:
+            dt = t_end - t
+        o.step_uniform(dt)
+        t += dt
+        ns += 1
+        if (t_end > 0.0 and t >= t_end * (1.0 - 1e-12)) or (max_steps > 0 and ns >= max_steps):
+            return m.to_dense(m.uold, 1), t, ns
 
 
 def interpol_hydro(u1, interpol_var, interpol_type, smallr=1e-10):

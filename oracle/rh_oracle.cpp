@@ -887,6 +887,25 @@ double rh_oracle_cmpdt(const double* uu, const double* grav, double dx, const rh
   return cmpdt(u, grav, dx, *p, ndim);
 }
 
+// Smallest cmpdt over the cells of noct octs in the reference layout
+// (uold(1:8,1:5,1:noct)): the cell loop of courant_fine (hydro/courant_fine.f90:
+// 112-168) on a whole single-level box, in any ndim (the batch's 2D problems
+// take the two-direction sum).
+double rh_oracle_cmpdt_octs(const double* uold, long long noct, const double* grav, double dx,
+                            const rh_hydro_params* p, int ndim, int nthreads) {
+  double best = 1e300;
+#pragma omp parallel for num_threads(nthreads > 0 ? nthreads : 1) reduction(min : best) schedule(static)
+  for (long long o = 0; o < noct; ++o) {
+    for (int c = 0; c < 8; ++c) {
+      double u[5];
+      for (int v = 0; v < 5; ++v) u[v] = uold[o * 40 + v * 8 + c];
+      const double d = cmpdt(u, grav, dx, *p, ndim);
+      best = d < best ? d : best;
+    }
+  }
+  return best;
+}
+
 int rh_oracle_interpol_hydro(const double* u1, double* u2, int interpol_var, int interpol_type,
                              double smallr) {
   double a[35];

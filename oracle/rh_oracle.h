@@ -47,6 +47,11 @@ int rh_oracle_unsplit(int nn, const double* uin, double dx, double dt,
 double rh_oracle_cmpdt(const double* uu, const double* grav, double dx,
                        const rh_hydro_params* p, int ndim);
 
+/* Smallest cmpdt() over every cell of noct octs of uold(1:8,1:5,1:noct),
+ * in ndim directions (courant_fine's cell loop, hydro/courant_fine.f90:112-168). */
+double rh_oracle_cmpdt_octs(const double* uold, long long noct, const double* grav, double dx,
+                            const rh_hydro_params* p, int ndim, int nthreads);
+
 /* interpol_hydro() (interpol_hydro.f90:5-109): u1(0:6,1:5) -> u2(1:8,1:5),
  * both Fortran-ordered (first index fastest). */
 int rh_oracle_interpol_hydro(const double* u1, double* u2, int interpol_var,

@@ -40,8 +40,12 @@ std::mutex g_mu;
 double* g_scratch_addr[kMaxDevices] = {};
 
 // Device address of the scratch array on the current device (host code only
-// sees a host-side stand-in under the array's name).
-int scratch_address(double** out) {
+// sees a host-side stand-in under the array's name).  Looked up again on every
+// call made outside stream capture, so an address cached before a device
+// reset (a new context, with the array at a new address) is never used by an
+// uncaptured call; a call on a stream that is being captured uses the address
+// of the last uncaptured call on that device, and fails if there was none.
+int scratch_address(cudaStream_t st, double** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return rh::cuda_fail(e, "cudaGetDevice");
@@ -49,12 +53,19 @@ int scratch_address(double** out) {
     rh::set_error("rh_cmpdt_noalloc: device ordinal %d beyond %d", dev, kMaxDevices);
     return RH_EINVAL;
   }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(st, &cs);
+  const bool capturing = e != cudaSuccess || cs != cudaStreamCaptureStatusNone;
+  if (e != cudaSuccess) (void)cudaGetLastError();  // the query's own error is not the caller's
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch_addr[dev]) {
+  if (!capturing) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return rh::cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
     g_scratch_addr[dev] = static_cast<double*>(p);
+  } else if (!g_scratch_addr[dev]) {
+    rh::set_error("rh_cmpdt_noalloc: the first call on device %d must be made outside stream capture", dev);
+    return RH_EINVAL;
   }
   *out = g_scratch_addr[dev];
   return RH_OK;
@@ -81,8 +92,9 @@ int rh_cmpdt_noalloc(const double* d_uold, int num_octs, const unsigned char* d_
     rh::set_error("rh_cmpdt_noalloc: need dx>0, gamma>1, smallc>0, courant_factor>0");
     return RH_EINVAL;
   }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
   double* scratch = nullptr;
-  int rc = scratch_address(&scratch);
+  int rc = scratch_address(st, &scratch);
   if (rc) return rc;
   rh::CflConst C;
   C.gamma = gamma;
@@ -99,7 +111,6 @@ int rh_cmpdt_noalloc(const double* d_uold, int num_octs, const unsigned char* d_
   C.ndim = 3;
   const long long ncell = (long long)num_octs * 8;
   const long long nblk = (ncell + kThreads - 1) / kThreads;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   rh::cmpdt_kernel<<<(unsigned)nblk, kThreads, 0, st>>>(d_uold, nullptr, 0, d_refined, 0, num_octs, C,
                                                          dx * dx * dx, scratch, nullptr);
   cudaError_t e = cudaGetLastError();

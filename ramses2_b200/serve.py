@@ -134,7 +134,9 @@ class HydroServer:
 
     def __init__(self, precision="fp32_bulk", pool_bytes=8 << 30, slope_type=2, riemann="hllc", tile=None,
                  chunk=4, keep_results=True, snapshot_dir=None):
-        """snapshot_dir: when set, every finished request leaves an output
+        """keep_results: True keeps every request's final state (Request.result),
+        False none, or a set of request ids whose states are kept.
+        snapshot_dir: when set, every finished request leaves an output
         directory ``<snapshot_dir>/req<rid>/output_00001`` in the reference's
         layout (amr and hydro files written from the device image, info.txt,
         hydro_header.txt) before its pool range is freed."""
@@ -190,7 +192,8 @@ class HydroServer:
                     r = active.pop(pid)
                     r.nsteps = int(nstep[pid])
                     r.t = float(tt[pid])
-                    if self.keep_results:
+                    keep = self.keep_results
+                    if keep is True or (keep and not isinstance(keep, bool) and r.rid in keep):
                         r.result = b.fetch(pid)
                     if self.snapshot_dir:
                         r.snapshot = b.write_output(pid, os.path.join(self.snapshot_dir, "req%05d" % r.rid), 1)

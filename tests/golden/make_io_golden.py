@@ -5,7 +5,7 @@ writers and decoded by the reference's own Python reader
 GridFile.read_level, leaf_cells).
 
 Run from the repository root with the reference checkout at REF_ROOT
-(default /root/reference):
+(default: oracle/Makefile's REF_ROOT):
 
     python tests/golden/make_io_golden.py
 
@@ -87,7 +87,9 @@ def read_with_reference(rio, m, img, time=0.125, nstep=7):
 
 
 def main():
-    ref_root = os.environ.get("REF_ROOT", "/root/reference")
+    ref_root = oracle.reference_root()
+    if ref_root is None:
+        sys.exit("reference checkout not found: set REF_ROOT")
     rio = ramses_io(ref_root)
     m = golden_mesh()
     img = images(m)

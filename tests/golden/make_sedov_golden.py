@@ -1,8 +1,9 @@
 """Generate tests/golden/sedov_analytic_3d.npz from the reference's own
 analytic Sedov solver (utils/py/sedov.py:4 sedovana), imported from the
-read-only reference checkout.  Run in the build container only:
+read-only reference checkout (argument, else REF_ROOT, else oracle/Makefile's
+REF_ROOT).  Run where the checkout exists:
 
-    python tests/golden/make_sedov_golden.py /root/reference
+    python tests/golden/make_sedov_golden.py [reference-root]
 
 The fixture holds the dimensionless self-similar profiles (r, d, u, p) for
 gamma = 1.4 and 1.6667 in 3D; scale with (E/rho0)^(1/5) t^(2/5) etc. as the
@@ -31,4 +32,14 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) > 1:
+        root = sys.argv[1]
+    else:
+        here = os.path.dirname(os.path.abspath(__file__))
+        sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(here)), "oracle"))
+        import oracle
+
+        root = oracle.reference_root()
+    if root is None:
+        sys.exit("reference checkout not found: set REF_ROOT or pass its path")
+    main(root)

@@ -16,7 +16,8 @@ from ramses2_b200.mesh import Mesh
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden", "io_amr3to5.npz")
-REF_IO = "/root/reference/utils/py/ramses_io.py"
+_REF = oracle.reference_root()
+REF_IO = os.path.join(_REF, "utils", "py", "ramses_io.py") if _REF else ""
 
 
 def fixture_mesh():

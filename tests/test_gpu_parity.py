@@ -349,6 +349,44 @@ def test_amr_coarse_step_native(bc, itype, ivar, spare):
         gpu.close()
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32_bulk"])
+def test_config1_form_amr_independent_runs_24_steps(prec):
+    """Config 1's form on a small mesh: Sedov on levels 3-5 refined by
+    hydro_refine's 0.1 gradient criteria (outflow, gamma 1.4, moncen, HLLC,
+    C = 0.8, interpol_type 1), 24 coarse steps with nsubcycle = 1.  The GPU
+    (rh_coarse_step, its own courant_fine dt) and the oracle evolve
+    independently; at every step the dt agrees to 1e-12 and the FP64 state
+    to 1e-12 relative L1 per variable (FP32-bulk: density 1e-5), so the
+    coarse-fine corrections and interpolated ghosts do not drift apart as
+    they compound."""
+    from ramses2_b200.mesh import sedov_amr_mesh
+
+    m, g = sedov_amr_mesh(3, 5, radius=0.3)
+    assert all(m.noct[l] for l in (3, 4, 5))
+    P = HydroParams.make(gamma=g, courant_factor=0.8, slope_type=2, riemann="hllc", interpol_var=0,
+                         interpol_type=1)
+    u0 = m.uold.copy()
+    o = oracle.OracleHydro(m, P, nthreads=NTHREADS)
+    dts, refs = [], []
+    for _ in range(24):
+        dts.append(amr_step(o, m))
+        refs.append(m.uold.copy())
+    m.uold[:] = u0
+    gpu = GodunovGPU(m, P, precision=prec)
+    try:
+        for s in range(24):
+            dt = gpu.coarse_step()
+            err = rel_l1(gpu.fetch_uold(), refs[s])
+            if prec == "fp64":
+                assert dt == pytest.approx(dts[s], rel=1e-12), s
+                assert np.all(err <= TOL_FP64), (s, err)
+            else:
+                assert dt == pytest.approx(dts[s], rel=1e-4), s
+                assert err[0] <= TOL_FP32_RHO, (s, err)
+    finally:
+        gpu.close()
+
+
 def test_amr_coarse_step_native_given_dt_fp32_bulk():
     """rh_coarse_step with the oracle's dt passed in (no courant_fine):
     FP32-bulk density within 1e-5 of the oracle's coarse step."""

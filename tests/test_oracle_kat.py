@@ -332,3 +332,41 @@ def test_amr_step_conserves_mass_and_energy_periodic():
     t1 = totals()
     assert t1[0] == pytest.approx(t0[0], rel=1e-13)
     assert t1[1] == pytest.approx(t0[1], rel=1e-13)
+
+
+# ---------------------------------------------------------------------------
+# Single-problem solver of the batch checks (oracle.solve_box)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_cmpdt_octs_is_the_cellwise_minimum(ndim):
+    rng = np.random.default_rng(11)
+    P = HydroParams.make(gamma=1.5, courant_factor=0.7)
+    noct = 37
+    rho = 10 ** rng.uniform(-2, 2, (noct, 8))
+    vel = rng.normal(0, 2, (3, noct, 8))
+    p = 10 ** rng.uniform(-3, 1, (noct, 8))
+    u = np.stack([rho, rho * vel[0], rho * vel[1], rho * vel[2],
+                  p / 0.5 + 0.5 * rho * (vel ** 2).sum(0)], axis=1)
+    want = min(oracle.cmpdt(u[o, :, c], 0.01, P, ndim=ndim) for o in range(noct) for c in range(8))
+    assert oracle.cmpdt_octs(u, 0.01, P, ndim=ndim, nthreads=NT) == want
+
+
+def test_solve_box_equals_level_stepping():
+    """A 16^3 box solved by solve_box for three steps is bitwise the same as
+    three step_uniform calls of a level-4 unit-box mesh (same cells, same
+    dx, same dt sequence)."""
+    m = uniform_mesh(4, nsubgrid=1, bc="outflow")
+    sedov3d(m, radius_cells=2.0)
+    P = HydroParams.make(gamma=1.4, courant_factor=0.8, slope_type=2, riemann="hllc")
+    dense0 = m.to_dense(m.uold, 4)
+    o = oracle.OracleHydro(m, P, nthreads=NT)
+    t = 0.0
+    for _ in range(3):
+        dt, _ = o.step_uniform()
+        t += dt
+    out, t_box, ns = oracle.solve_box(dense0, m.dx(4), P, bc="outflow", max_steps=3, nthreads=NT)
+    assert ns == 3 and t_box == t
+    assert np.array_equal(out, m.to_dense(m.uold, 4))
+    # with t_end the last step is cut to land on it
+    out2, t2, ns2 = oracle.solve_box(dense0, m.dx(4), P, bc="outflow", t_end=0.5 * t, nthreads=NT)
+    assert t2 == pytest.approx(0.5 * t, rel=1e-12) and ns2 <= 3

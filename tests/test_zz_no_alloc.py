@@ -60,6 +60,59 @@ def test_noalloc_cmpdt_matches_rh_cmpdt_on_two_calls():
         gpu.close()
 
 
+def test_noalloc_cmpdt_amr_levels_with_refined_mask_on_a_stream():
+    """Each level of a three-level mesh through rh_cmpdt_noalloc with the
+    level's refined-cell mask (refined cells are skipped), on a stream of the
+    caller's, twice: the same values as rh_cmpdt, and no device memory taken
+    by the second call."""
+    import torch
+
+    from ramses2_b200.mesh import amr_mesh, fill_amr_prim
+
+    L = lib()
+    f = _bind(L)
+    m = amr_mesh(3, 5, lambda x, l: np.sqrt(((x - 0.5) ** 2).sum(-1)) < 0.2, bc="outflow")
+
+    def prim(x, l):
+        r = np.sqrt(((x - 0.5) ** 2).sum(-1))
+        return 1 + 0.5 * np.exp(-r ** 2 / 0.02), 0.3 + 0 * r, -0.2 + 0.1 * x[..., 0], 0.1 + 0 * r, 1 + np.exp(-r ** 2 / 0.01)
+
+    fill_amr_prim(m, prim, 1.4)
+    P = HydroParams.make(gamma=1.4, courant_factor=0.8, slope_type=2, riemann="hllc")
+    grav = np.zeros(3)
+    gpu = GodunovGPU(m, P, precision="fp64")
+    side = torch.cuda.Stream()
+    try:
+        uold = C.c_void_p()
+        assert L.rh_state_ptrs(C.byref(uold), None, None, None) == 0
+        out = torch.empty(5, dtype=torch.float64, device="cuda")
+        checked_refined = False
+        for lev in range(m.levelmin, m.levelmax + 1):
+            sl = m.level_slice(lev)
+            refined = np.ascontiguousarray((m.grid[sl]["refined"] != 0).astype(np.uint8))
+            checked_refined |= bool(refined.any())
+            d_ref = torch.from_numpy(refined.reshape(-1)).to("cuda")
+            expected = gpu.courant_fine(lev)
+            gpu.sync()
+            base = uold.value + (int(m.head[lev]) - 1) * 320
+            for call in range(2):
+                out.fill_(-1.0)
+                torch.cuda.synchronize()
+                free0 = torch.cuda.mem_get_info()[0]
+                rc = f(C.c_void_p(base), int(m.noct[lev]), C.c_void_p(d_ref.data_ptr()), m.dx(lev), P.gamma,
+                       P.smallr, P.smallc, P.courant_factor, grav.ctypes.data_as(C.POINTER(C.c_double)),
+                       C.c_void_p(out.data_ptr()), C.c_void_p(side.cuda_stream))
+                assert rc == 0, L.rh_last_error().decode()
+                side.synchronize()
+                if call == 1:
+                    assert torch.cuda.mem_get_info()[0] == free0
+                got = out.cpu().numpy()
+                np.testing.assert_allclose(got[[0, 1, 2, 4]], expected[[0, 1, 2, 4]], rtol=1e-12)
+        assert checked_refined
+    finally:
+        gpu.close()
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     L = lib()
     f = _bind(L)
