@@ -37,6 +37,7 @@ extern "C" {
 #define RH_ETIMEDOUT   5   /* bounded device wait gave up                  */
 #define RH_ENODEV      6   /* no CUDA device / extension not built          */
 #define RH_EBUSY       7   /* serving queue full                           */
+#define RH_EBADSTATE   8   /* state check found NaN/Inf, rho<=0 or eint<=0 */
 
 /* Riemann solver ids: hydro/hydro_parameters.f90:30-32 */
 #define RH_RIEMANN_LLF  1

@@ -61,8 +61,9 @@ int rh_batch_add(const rh_batch_problem* p, const rh_batch_ic* ic, int* id);
 int rh_batch_remove(int id);
 /* Advance every unfinished problem by nsteps steps (graph replays). */
 int rh_batch_step(int nsteps);
-/* Per-problem state: time, steps taken, done flag, current dt and the
- * courant_fine totals (mass, ekin, eint, emag, dt) of the current state. */
+/* Per-problem state: time, steps taken, done flag (0 running, 1 finished,
+ * 2 stopped by the state check), current dt and the courant_fine totals
+ * (mass, ekin, eint, emag, dt) of the current state. */
 int rh_batch_status(int id, double* t, int* nstep, int* done, double* dt, double* totals5);
 /* Status of every problem slot at once (arrays of rh_batch_capacity()). */
 int rh_batch_poll(int* done, int* nstep, double* t);
@@ -86,6 +87,14 @@ long long rh_batch_cells(void);
  * bit (the pencil body's z terms are exact zeros there); the choice is kept for
  * that comparison. */
 int rh_batch_set_plane_path(int on);
+/* on != 0: after each step every stepped problem's new state is checked as
+ * rh_check_state checks a level (NaN/Inf, density <= 0, internal energy <= 0;
+ * gpu/gpu_utils.cuf:90-118, hydro/godunov_utils.f90:278-287), and a problem
+ * with a bad cell is stopped with done = 2 (the others go on).  Off by
+ * default: one extra read of the stepped states per step. */
+int rh_batch_set_state_check(int on);
+/* The check's bits of a problem (1 NaN/Inf, 2 rho <= 0, 4 eint <= 0), 0 if clean. */
+int rh_batch_check_mask(int id, int* mask);
 
 #ifdef __cplusplus
 }

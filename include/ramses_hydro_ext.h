@@ -54,6 +54,23 @@ int rh_level_ghosts(int ilevel, int* gsrc_oct, unsigned char* gsrc_cf, int* gfat
  * Godunov step reads a level that an earlier set_uold or restriction of the
  * step would have changed. */
 int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl);
+
+/* Device state check of one level's current uold, the reference's debug scan
+ * after set_uold (check_nan_kernel, gpu/gpu_utils.cuf:90-118, called by
+ * gpu_check_nan, gpu/gpu_runner.cuf:5316-5391) extended by cmpdt's
+ * negative-pressure stop (hydro/godunov_utils.f90:278-287).  Every cell of
+ * octs head_idx .. head_idx+num_octs-1 (1-based) is tested; *nbad receives
+ * the number of bad cells, *first_oct the smallest bad oct index (1-based,
+ * 0 when none) and *mask the OR of: 1 NaN or Inf in a conserved variable,
+ * 2 density <= 0, 4 internal energy E - |rho u|^2/(2 rho) <= 0 at positive
+ * density.  Where the reference prints the oct and stops the run, the host
+ * decides.  Synchronous. */
+int rh_check_state(int head_idx, int num_octs, int* nbad, int* first_oct, int* mask);
+/* on != 0: rh_coarse_step runs that check on every level after the step
+ * (the reference's gpu_debug switch) and returns RH_EBADSTATE, the level,
+ * count, first oct and mask in rh_last_error(), when a cell is bad.  Off by
+ * default (one extra read of the state per coarse step). */
+int rh_set_state_check(int on);
 /* Where rh_set_mesh builds coarse-fine tables: 1 on the device (default),
  * 0 on the host (the reference builder the device one is tested against). */
 int rh_set_table_builder(int on_device);
@@ -112,6 +129,11 @@ int rh_cmpdt_noalloc(const double* d_uold, int num_octs, const unsigned char* d_
  * word rh_sync reads, with the context still usable.  For tests of the
  * failure path; faults, traps and hangs are never used. */
 int rh_selftest_wait(long long bound);
+/* For tests of the pencil kernels' FP64 lane arithmetic: for n device doubles
+ * x, writes d_out[0:n] = the kernels' reciprocal (vrcp), d_out[n:2n] = their
+ * square root (vsqrt), d_out[2n:3n] = CUDA's 1.0/x and d_out[3n:4n] = CUDA's
+ * sqrt(x).  Synchronous. */
+int rh_selftest_vmath(const double* d_x, long long n, double* d_out);
 
 #ifdef __cplusplus
 }

@@ -6,7 +6,10 @@
 // trace + Riemann pipeline (trace_3d, riemann_driver: one threadgroup with
 // one thread) to the tests, which compare them with the FP64 oracle at FP32
 // precision.  The shader source is included from the reference checkout by the
-// recipe (HYDRO_METAL); nothing of it is copied here.
+// recipe (HYDRO_METAL); nothing of it is copied here.  Built twice: as the
+// shader is (float32, librh_ref_msl.so) and with RH_MSL_DOUBLE (every float of
+// the shader and of the functions below is double, librh_ref_msl64.so), which
+// pins the oracle to the shader's algorithm at FP64 rounding.
 #include HYDRO_METAL
 
 extern "C" {
@@ -109,7 +112,7 @@ int ref_msl_cmpdt(const oct_t* grid, const float* uold, int head_idx, int num_oc
                   float smallr, float smallc2, float courant, const float* grav, float* out) {
   metal::atomic_uint data[5];
   for (int i = 0; i < 4; ++i) data[i].v = 0u;
-  data[4].v = metal::as_type<unsigned int>(HUGE_VALF);
+  data[4].v = metal::as_type<uint>((float)HUGE_VAL);  // +inf of the build's float (double in the FP64 build)
   const long long nthreads = (long long)num_octs * TWOTONDIM;
   for (long long t = 0; t < nthreads; ++t)
     cmpdt_kernel(grid, uold, data, head_idx, num_octs, dx, gamma, smallr, smallc2, courant, grav, nullptr,

@@ -30,6 +30,7 @@ STATUS = {
     5: "RH_ETIMEDOUT",
     6: "RH_ENODEV",
     7: "RH_EBUSY",
+    8: "RH_EBADSTATE",
 }
 
 

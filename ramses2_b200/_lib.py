@@ -49,6 +49,9 @@ SIGNATURES = {
     "rh_timer_start": (_i, []),
     "rh_timer_stop": (_i, [_P(C.c_float)]),
     "rh_selftest_wait": (_i, [C.c_longlong]),
+    "rh_selftest_vmath": (_i, [C.c_void_p, C.c_longlong, C.c_void_p]),
+    "rh_check_state": (_i, [_i, _i, _P(_i), _P(_i), _P(_i)]),
+    "rh_set_state_check": (_i, [_i]),
     # restart / snapshot files (include/ramses_hydro_io.h)
     "rh_file_size": (_i, [_i, _P(C.c_longlong)]),
     "rh_file_image": (_i, [_i, _d, C.c_void_p, C.c_longlong, _P(C.c_longlong)]),
@@ -71,6 +74,8 @@ SIGNATURES = {
     "rh_batch_bench": (_i, [_i, _P(C.c_float)]),
     "rh_batch_cells": (C.c_longlong, []),
     "rh_batch_set_plane_path": (_i, [_i]),
+    "rh_batch_set_state_check": (_i, [_i]),
+    "rh_batch_check_mask": (_i, [_i, _P(_i)]),
 }
 
 

@@ -202,6 +202,17 @@ class Batch:
         check(self.L.rh_batch_bench(int(nsteps), C.byref(ms)), "rh_batch_bench")
         return ms.value
 
+    def set_state_check(self, on=True):
+        """Check every stepped problem after each step; a problem with a NaN/Inf,
+        rho <= 0 or internal energy <= 0 cell stops with done == 2."""
+        check(self.L.rh_batch_set_state_check(int(bool(on))), "rh_batch_set_state_check")
+
+    def check_mask(self, pid):
+        """The state check's bits of a problem (0: clean)."""
+        m = C.c_int()
+        check(self.L.rh_batch_check_mask(int(pid), C.byref(m)), "rh_batch_check_mask")
+        return m.value
+
     def cells(self):
         """Cells one step updates (unfinished problems)."""
         return int(self.L.rh_batch_cells())

@@ -387,6 +387,7 @@ int rh_finalize(void) {
   rh_batch_free();
   free_state();
   cudaFree(c.d_err);
+  cudaFree(c.d_check);
   cudaFreeHost(c.h_cfl);
   cudaEventDestroy(c.ev0);
   cudaEventDestroy(c.ev1);
@@ -1200,6 +1201,7 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
     }
   }
   *dt = step_dt;
+  if (c.state_check) return check_all_levels();  // the reference's gpu_debug scan after set_uold
   return RH_OK;
 }
 

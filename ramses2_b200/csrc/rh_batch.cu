@@ -10,6 +10,7 @@
 #include "ramses_hydro_batch.h"
 #include "ramses_hydro_io.h"
 #include "rh_batch.cuh"
+#include "rh_check.cuh"
 #include "rh_internal.h"
 
 namespace rh {
@@ -79,6 +80,11 @@ struct Batch {
   int nblocks = 0;
   double* d_tmp = nullptr;       // initial-CFL partials
   long long tmp_cap = 0;
+  // state check after each step (rh_batch_set_state_check)
+  int check = 0;
+  int* d_bad = nullptr;          // [cap] OR of the check's bits per problem
+  long long* d_coff = nullptr;   // [cap+1] first check block of each work-list slot
+  long long nchunk = 0;          // check blocks (32 octs each) over the work list
 };
 
 Batch& B() {
@@ -185,6 +191,30 @@ __device__ __forceinline__ double next_dt(const BatchProb& P, double t, double c
   return dt;
 }
 
+// Device state check of the problems stepped this step (done == 0 before the
+// reduction): block b checks 32 octs of the problem in slot s with
+// coff[s] <= b < coff[s+1], in the pool buffer the step wrote; the bits of
+// cell_state_bits are OR-ed into bad[id].
+__global__ void batch_check_kernel(const BatchProb* __restrict__ prob, const int* __restrict__ order,
+                                   const long long* __restrict__ coff, int nslot, const int* __restrict__ done,
+                                   const double* ud, const float* uf, int fp32, int* __restrict__ bad) {
+  const long long blk = blockIdx.x;
+  int lo = 0, hi = nslot - 1;
+  while (lo < hi) {  // the last slot whose first block is <= blk
+    const int mid = (lo + hi + 1) >> 1;
+    if (coff[mid] <= blk) lo = mid;
+    else hi = mid - 1;
+  }
+  const int id = order[lo];
+  if (done[id]) return;
+  const BatchProb& P = prob[id];
+  const long long noct = (long long)(P.ncx >> 1) * (P.ncy >> 1) * (P.ncz >> 1);
+  const long long o = (blk - coff[lo]) * 32 + (threadIdx.x >> 3);
+  if (o >= noct) return;
+  const unsigned bits = load_cell_bits(ud, uf, fp32, P.oct0 + o, (int)(threadIdx.x & 7));
+  if (bits) atomicOr(&bad[id], (int)bits);
+}
+
 // Reduce the partials of n blocks into totals and (optionally) advance time.
 __device__ void reduce_block(const double* partial, long long n, double* out4) {
   __shared__ double red[256][4];
@@ -226,7 +256,7 @@ __global__ void batch_init_dt_kernel(BatchProb P, int id, const double* partial,
 // order), advance t and the step count, set the next dt and the done flag.
 __global__ void batch_reduce_kernel(const BatchProb* prob, const int* order, const long long* woff,
                                     const double* partial, int* done, int* nstep, int* cur, double* dt, double* t,
-                                    double* tot, unsigned long long* counter, int parity) {
+                                    double* tot, unsigned long long* counter, int parity, const int* bad) {
   const int slot = blockIdx.x;
   const int id = order[slot];
   if (slot == 0 && threadIdx.x == 0) *counter = 0ull;
@@ -243,7 +273,7 @@ __global__ void batch_reduce_kernel(const BatchProb* prob, const int* order, con
     double* o = tot + id * 5ll;
     o[0] = r4[0]; o[1] = r4[1]; o[2] = r4[2]; o[3] = 0.0; o[4] = r4[3];
     const bool fin = (P.t_end > 0.0 && tn >= P.t_end * (1.0 - 1e-12)) || (P.max_steps > 0 && ns >= P.max_steps);
-    done[id] = fin ? 1 : 0;
+    done[id] = bad[id] ? 2 : (fin ? 1 : 0);  // 2: stopped by the state check
     dt[id] = next_dt(P, tn, r4[3]);
   }
 }
@@ -306,6 +336,16 @@ BatchProb make_prob(const rh_batch_problem& p, long long oct0) {
   return P;
 }
 
+// The state check of the step of the given parity (its new state is in pool
+// buffer 1 - parity), when switched on.
+void check_step(int parity) {
+  Batch& b = B();
+  if (!b.check || b.nchunk == 0) return;
+  batch_check_kernel<<<(unsigned)b.nchunk, 256, 0, ctx().stream>>>(
+      b.d_prob, b.d_order, b.d_coff, b.nslot, b.d_done, b.ud[1 - parity], b.uf[1 - parity],
+      b.precision == RH_PREC_FP32_BULK ? 1 : 0, b.d_bad);
+}
+
 // Rebuild the work list (largest problems first) and the step graph.
 int rebuild() {
   Batch& b = B();
@@ -325,6 +365,11 @@ int rebuild() {
   }
   b.nslot = (int)ids.size();
   b.nwork = woff.back();
+  std::vector<long long> coff(ids.size() + 1, 0);
+  for (size_t s = 0; s < ids.size(); ++s) coff[s + 1] = coff[s] + (b.probs[ids[s]].noct + 31) / 32;
+  b.nchunk = coff.back();
+  RH_CUDA(cudaMemcpyAsync(b.d_coff, coff.data(), sizeof(long long) * coff.size(), cudaMemcpyHostToDevice,
+                          c.stream));
   RH_CUDA(cudaMemcpyAsync(b.d_prob, probs.data(), sizeof(BatchProb) * b.cap, cudaMemcpyHostToDevice, c.stream));
   if (!ids.empty())
     RH_CUDA(cudaMemcpyAsync(b.d_order, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice, c.stream));
@@ -373,9 +418,10 @@ int rebuild() {
         cudaStreamEndCapture(c.stream, &g);
         return cuda_fail(e, "batch step capture");
       }
+      check_step(par);
       batch_reduce_kernel<<<b.nslot, 256, 0, c.stream>>>(b.d_prob, b.d_order, b.d_woff, b.d_partial, b.d_done,
                                                          b.d_nstep, b.d_cur, b.d_dt, b.d_t, b.d_tot, b.d_counter,
-                                                         par);
+                                                         par, b.d_bad);
     }
     RH_CUDA(cudaStreamEndCapture(c.stream, &g));
     bool updated = false;
@@ -442,6 +488,9 @@ int rh_batch_init(int precision, int slope, int riemann, long long pool_octs) {
   RH_CUDA(cudaMalloc(&b.d_order, sizeof(int) * b.cap));
   RH_CUDA(cudaMalloc(&b.d_woff, sizeof(long long) * (b.cap + 1)));
   RH_CUDA(cudaMalloc(&b.d_counter, sizeof(unsigned long long)));
+  RH_CUDA(cudaMalloc(&b.d_bad, sizeof(int) * b.cap));
+  RH_CUDA(cudaMalloc(&b.d_coff, sizeof(long long) * (b.cap + 1)));
+  RH_CUDA(cudaMemset(b.d_bad, 0, sizeof(int) * b.cap));
   RH_CUDA(cudaMemset(b.d_counter, 0, sizeof(unsigned long long)));
   RH_CUDA(cudaMemset(b.d_done, 0, sizeof(int) * b.cap));
   b.probs.assign(b.cap, HostProb());
@@ -472,6 +521,8 @@ int rh_batch_free(void) {
   cudaFree(b.d_partial);
   cudaFree(b.d_counter);
   cudaFree(b.d_tmp);
+  cudaFree(b.d_bad);
+  cudaFree(b.d_coff);
   b = Batch();
   return RH_OK;
 }
@@ -564,6 +615,7 @@ int rh_batch_add(const rh_batch_problem* p, const rh_batch_ic* ic, int* id) {
     const double dz = 0.0;
     if ((e = cudaMemcpyAsync(b.d_done + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, c.stream)) ||
         (e = cudaMemcpyAsync(b.d_nstep + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, c.stream)) ||
+        (e = cudaMemcpyAsync(b.d_bad + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, c.stream)) ||
         (e = cudaMemcpyAsync(b.d_cur + slot, &b.parity, sizeof(int), cudaMemcpyHostToDevice, c.stream)) ||
         (e = cudaMemcpyAsync(b.d_t + slot, &dz, sizeof(double), cudaMemcpyHostToDevice, c.stream)))
       return e;
@@ -650,9 +702,10 @@ int rh_batch_step(int nsteps) {
                   b.d_done, b.d_dt, b.d_partial, {b.ud[0], b.ud[1]}, {b.uf[0], b.uf[1]}, c.d_err,
                   b.plane2d};
       RH_CUDA(reg->fn(A, b.parity, b.nblocks, c.stream));
+      check_step(b.parity);
       batch_reduce_kernel<<<b.nslot, 256, 0, c.stream>>>(b.d_prob, b.d_order, b.d_woff, b.d_partial, b.d_done,
                                                          b.d_nstep, b.d_cur, b.d_dt, b.d_t, b.d_tot, b.d_counter,
-                                                         b.parity);
+                                                         b.parity, b.d_bad);
       RH_CUDA(cudaGetLastError());
       b.parity ^= 1;
       done_steps += 1;
@@ -675,6 +728,28 @@ int rh_batch_status(int id, double* t, int* nstep, int* done, double* dt, double
   if (done) RH_CUDA(cudaMemcpy(done, b.d_done + id, sizeof(int), cudaMemcpyDeviceToHost));
   if (dt) RH_CUDA(cudaMemcpy(dt, b.d_dt + id, sizeof(double), cudaMemcpyDeviceToHost));
   if (totals5) RH_CUDA(cudaMemcpy(totals5, b.d_tot + id * 5ll, 5 * sizeof(double), cudaMemcpyDeviceToHost));
+  return RH_OK;
+}
+
+int rh_batch_set_state_check(int on) {
+  Batch& b = B();
+  if (!b.inited) {
+    set_error("rh_batch_init has not been called");
+    return RH_ESTATE;
+  }
+  b.check = on ? 1 : 0;
+  b.dirty = true;  // the step graph gains or loses the check kernel
+  return RH_OK;
+}
+
+int rh_batch_check_mask(int id, int* mask) {
+  Batch& b = B();
+  if (!b.inited || id < 0 || id >= b.cap || !b.probs[id].used || !mask) {
+    set_error("rh_batch_check_mask: no problem %d", id);
+    return RH_EINVAL;
+  }
+  RH_CUDA(cudaStreamSynchronize(ctx().stream));
+  RH_CUDA(cudaMemcpy(mask, b.d_bad + id, sizeof(int), cudaMemcpyDeviceToHost));
   return RH_OK;
 }
 

@@ -58,6 +58,7 @@ struct Context {
   TileCfg amr_cfg{8, 4, 2, 8};  // tiles of multi-level meshes (coarse-fine kernels)
   bool amr_cfg_set = false;     // amr_cfg chosen by rh_set_amr_tile (else by precision at rh_set_mesh)
   int table_builder = 1;        // coarse-fine tables: 1 on the device, 0 on the host
+  int state_check = 0;          // rh_coarse_step checks every level after set_uold (rh_set_state_check)
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
@@ -86,6 +87,8 @@ struct Context {
   std::vector<int2*> d_face;       // per level: [noct][6] cells across each face (rh_hydro_flag)
   int nlevels_used = 0;
   int* d_err = nullptr;
+  unsigned* d_check = nullptr;    // [levelmax+1][3] state check results (rh_check.cu)
+  int check_cap = 0;
   double* d_cfl = nullptr;        // [levelmax+1][5] reduced CFL values
   double* d_scratch = nullptr;    // standalone cmpdt partials
   double* h_cfl = nullptr;        // pinned: courant_fine values read back, 5 per level
@@ -115,6 +118,9 @@ int prolong_ghosts(int l, double smallr);
 int build_amr_tables_device(int l, const TileCfg& cfg, long long gbase, const rh_oct* d_grid, int2** d_gfather_out);
 // complete levels (rh_tables.cu)
 int build_complete_tables_device(int l, const TileCfg& cfg, LevelTables& T);
+
+// device state check of every level (rh_check.cu): RH_EBADSTATE on a bad cell
+int check_all_levels();
 
 // restart / snapshot file images (rh_io.cu)
 struct ImageSrc {

@@ -91,6 +91,20 @@ class GodunovGPU:
                                    flag1.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(n)), "rh_hydro_flag")
         return n.value
 
+    def check_state(self, ilevel):
+        """The reference's debug scan of a level's uold (gpu_check_nan):
+        (bad cells, first bad oct 1-based or 0, mask: 1 NaN/Inf, 2 rho<=0,
+        4 internal energy<=0)."""
+        m = self.mesh
+        nbad, first, mask = C.c_int(), C.c_int(), C.c_int()
+        check(self.L.rh_check_state(int(m.head[ilevel]), int(m.noct[ilevel]), C.byref(nbad), C.byref(first),
+                                    C.byref(mask)), "rh_check_state")
+        return nbad.value, first.value, mask.value
+
+    def set_state_check(self, on=True):
+        """Make coarse_step check every level after the step (RH_EBADSTATE)."""
+        check(self.L.rh_set_state_check(int(bool(on))), "rh_set_state_check")
+
     # ---- conveniences -----------------------------------------------------------
     def step_uniform(self, dt=None):
         """One coarse step of a single-level run in the reference's order."""

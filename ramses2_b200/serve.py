@@ -40,6 +40,7 @@ class Request:
     result: np.ndarray = field(default=None, repr=False)
     snapshot: str = None
     rejected: bool = False
+    failed: int = 0            # state check bits when the solve was stopped (1 NaN/Inf, 2 rho<=0, 4 eint<=0)
 
     @property
     def cells(self):
@@ -133,9 +134,13 @@ class HydroServer:
     """Continuous-batching server over one device pool of ``pool_bytes``."""
 
     def __init__(self, precision="fp32_bulk", pool_bytes=8 << 30, slope_type=2, riemann="hllc", tile=None,
-                 chunk=4, keep_results=True, snapshot_dir=None):
+                 chunk=4, keep_results=True, snapshot_dir=None, state_check=False):
         """keep_results: True keeps every request's final state (Request.result),
         False none, or a set of request ids whose states are kept.
+        state_check: check every stepped state on the device after each step
+        (rh_batch_set_state_check); a request whose state goes bad (NaN/Inf,
+        rho <= 0, internal energy <= 0) is stopped and reported failed
+        (Request.failed holds the bits) instead of returning garbage.
         snapshot_dir: when set, every finished request leaves an output
         directory ``<snapshot_dir>/req<rid>/output_00001`` in the reference's
         layout (amr and hydro files written from the device image, info.txt,
@@ -146,6 +151,8 @@ class HydroServer:
         self.batch = Batch(precision, slope_type=slope_type, riemann=riemann, pool_octs=self.pool_octs, tile=tile)
         self.chunk = int(chunk)
         self.keep_results = keep_results
+        if state_check:
+            self.batch.set_state_check(True)
 
     def close(self):
         self.batch.close()
@@ -192,6 +199,8 @@ class HydroServer:
                     r = active.pop(pid)
                     r.nsteps = int(nstep[pid])
                     r.t = float(tt[pid])
+                    if done[pid] == 2:
+                        r.failed = b.check_mask(pid)
                     keep = self.keep_results
                     if keep is True or (keep and not isinstance(keep, bool) and r.rid in keep):
                         r.result = b.fetch(pid)
@@ -199,17 +208,19 @@ class HydroServer:
                         r.snapshot = b.write_output(pid, os.path.join(self.snapshot_dir, "req%05d" % r.rid), 1)
                     b.remove(pid)
                     r.finished = now()
-                    updates += r.solved_cells * r.nsteps
+                    if not r.failed:
+                        updates += r.solved_cells * r.nsteps
                     if log:
                         log("req %d %s %s done: %d steps, latency %.3f s" % (r.rid, r.kind, tuple(r.prob.n),
                                                                              r.nsteps, r.latency))
         makespan = now()
-        served = [r for r in requests if not r.rejected]
+        served = [r for r in requests if not r.rejected and not r.failed]
         lat = np.array([r.latency for r in served])
         return {
             "requests": len(requests),
             "served": len(served),
             "rejected": sum(r.rejected for r in requests),
+            "failed": sum(bool(r.failed) for r in requests),
             "makespan_s": makespan,
             "cell_updates": int(updates),
             "cell_updates_per_s": updates / makespan if makespan > 0 else 0.0,
