@@ -11,8 +11,11 @@ gpu_cmpdt_2), rh_set_unew, rh_godunov, rh_set_uold.
 
 value        cell-updates/s of the FP32-bulk step (state resident in HBM)
 fp64         the same for the plain FP64 step
-e2e          FP32-bulk step with host buffers: per step rh_set_grid_device
-             from pinned host memory and rh_transfer_grid_host back
+e2e          FP32-bulk step with the reference's FP64 uold in pinned host
+             memory, copied in and out every step: rh_coarse_step_host (the
+             copies overlapped with the pencils); beside it the three
+             separate calls rh_set_grid_device, rh_coarse_step,
+             rh_transfer_grid_host
 roofline     dominant kernel (godunov_pencil_kernel), algorithmic bytes per
              cell-update (48 B FP32-bulk, 80 B FP64) / CUDA-event kernel time
 cpu_baseline the CPU restatement of the reference path (oracle/, OpenMP over
@@ -533,8 +536,9 @@ def bench_sedov512(args, rank, world, dist, device, tuned):
 
 def bench_turbulence(args, rank, world, dist, device):
     """Config-2: decaying supersonic turbulence on 256^3 (gamma 1.001, rms
-    Mach 5, lognormal density, minmod, HLLC, periodic), args.turb_steps
-    FP32-bulk and FP64 steps; FP32-bulk relative L1 against FP64 after them."""
+    Mach 5, lognormal density, minmod, HLLC, periodic), tiles autotuned on
+    this state, args.turb_steps FP32-bulk and FP64 steps; FP32-bulk relative
+    L1 against FP64 after them."""
     from ramses2_b200._abi import HydroParams
     from ramses2_b200._lib import lib
     from ramses2_b200.hydro import GodunovGPU
@@ -550,10 +554,14 @@ def bench_turbulence(args, rank, world, dist, device):
     out = {"workload": "decaying turbulence 256^3, gamma 1.001, rms Mach 5, minmod, HLLC",
            "cells": ncell, "steps": args.turb_steps}
     final = {}
+    from ramses2_b200 import autotune
+
     for prec in ("fp64", "fp32_bulk"):
         m.uold[:] = u0
         gpu = GodunovGPU(m, P, precision=prec, device=device)
-        gpu.coarse_step()
+        dt0 = gpu.coarse_step()
+        best, _ = autotune.tune(gpu, LEVEL, dt0)  # tiles tuned on this workload itself
+        out.setdefault("tile", {})[prec] = best
         gpu.push_uold(u0)
         ms = _timed(L, lambda: [gpu.coarse_step() for _ in range(args.turb_steps)]) / args.turb_steps
         final[prec] = gpu.fetch_uold()
@@ -622,6 +630,7 @@ def run_ours(args):
             host[:] = u0
             from ramses2_b200._abi import dptr
 
+            # the three separate calls (upload, step, read back), one after the other
             gpu.sync()
             check(L.rh_timer_start(), "rh_timer_start")
             for _ in range(args.steps):
@@ -630,7 +639,21 @@ def run_ours(args):
                 check(L.rh_transfer_grid_host(dptr(host), m.ngridmax, 5, 8), "rh_transfer_grid_host")
             e2e_ms = C.c_float()
             check(L.rh_timer_stop(C.byref(e2e_ms)), "rh_timer_stop")
+            results["e2e_serial_ms"] = e2e_ms.value / args.steps
+            # rh_coarse_step_host: the copies overlapped with the pencils; each
+            # call takes the dt_next its predecessor returned
+            host[:] = u0
+            _, nxt = gpu.coarse_step_host(host)
+            for _ in range(args.warmup - 1):
+                _, nxt = gpu.coarse_step_host(host, dt=nxt)
+            check(L.rh_timer_start(), "rh_timer_start")
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                _, nxt = gpu.coarse_step_host(host, dt=nxt)
+            wall = time.perf_counter() - t0
+            check(L.rh_timer_stop(C.byref(e2e_ms)), "rh_timer_stop")
             results["e2e_ms"] = e2e_ms.value / args.steps
+            results["e2e_wall_ms"] = wall * 1e3 / args.steps
             results["e2e_bytes"] = int(m.uold.nbytes)
         gpu.close()
     s512 = bench_sedov512(args, rank, world, dist, device, tuned) if args.sedov512_steps > 0 else None
@@ -642,8 +665,10 @@ def run_ours(args):
     if dist is not None:
         from ramses2_b200.ranks import max_over_ranks
 
-        results["fp32_bulk"]["ms_per_step"], results["fp64"]["ms_per_step"], results["e2e_ms"] = max_over_ranks(
-            [results["fp32_bulk"]["ms_per_step"], results["fp64"]["ms_per_step"], results["e2e_ms"]], dist)
+        (results["fp32_bulk"]["ms_per_step"], results["fp64"]["ms_per_step"], results["e2e_ms"],
+         results["e2e_serial_ms"]) = max_over_ranks(
+            [results["fp32_bulk"]["ms_per_step"], results["fp64"]["ms_per_step"], results["e2e_ms"],
+             results["e2e_serial_ms"]], dist)
     if rank != 0:
         if dist is not None:
             dist.barrier()
@@ -773,7 +798,11 @@ def run_ours(args):
                             "p99": float(np.percentile(results[prec]["per_step"], 99))},
         "tile": {k: v for k, v in tuned.items()},
         "e2e": {"value": world * ncell / (results["e2e_ms"] * 1e-3), "unit": "cell-updates/s",
-                "h2d_bytes_per_step": results["e2e_bytes"], "d2h_bytes_per_step": results["e2e_bytes"]},
+                "h2d_bytes_per_step": results["e2e_bytes"], "d2h_bytes_per_step": results["e2e_bytes"],
+                "call": "rh_coarse_step_host (FP64 uold in pinned host memory, in and out every step)",
+                "ms_per_step": results["e2e_ms"], "wall_ms_per_step": results["e2e_wall_ms"],
+                "serial_calls_cell_updates_per_s": world * ncell / (results["e2e_serial_ms"] * 1e-3),
+                "serial_calls_ms_per_step": results["e2e_serial_ms"]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": profile_traffic(prec), "peak_kind": peak_kind,
                      "kernel": "godunov_pencil2_kernel (FP32-bulk)", "kernel_ms": kms,

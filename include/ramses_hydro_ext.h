@@ -55,6 +55,25 @@ int rh_level_ghosts(int ilevel, int* gsrc_oct, unsigned char* gsrc_cf, int* gfat
  * step would have changed. */
 int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl);
 
+/* One coarse step of a mesh whose uold lives in host memory: host_in (the
+ * reference layout uold(1:8,1:5,1:ngridmax)) is copied to the device, stepped
+ * as rh_coarse_step steps it, and the new state is written to host_out (may
+ * be host_in).  No counterpart in the reference, whose GPU runner keeps uold
+ * on the device between steps; this is for hosts that hand over their state
+ * every step.  On a single-level mesh the two copies and the Godunov pencils
+ * overlap chunk by chunk (a pencil runs once its neighbourhood has arrived, a
+ * chunk is read back once the pencils writing it are done), with the new
+ * state and dt_next bitwise those of rh_set_grid_device + rh_coarse_step +
+ * rh_transfer_grid_host (the cached conserved totals to rounding); other
+ * meshes make those three calls.  *dt > 0 on entry is the step's dt
+ * (else courant_fine of host_in, after the whole upload); *dt receives the dt
+ * taken and *dt_next (optional) min(dx/smallc, courant dt) of the new state,
+ * from the step's fused CFL epilogue: a host that loops passes it back as the
+ * next call's dt, which lets the upload overlap the pencils.  Host buffers
+ * should be pinned (cudaHostAlloc) for the copies to overlap. */
+int rh_coarse_step_host(const rh_hydro_params* p, const double* host_in, double* host_out, double* dt,
+                        double* dt_next);
+
 /* Device state check of one level's current uold, the reference's debug scan
  * after set_uold (check_nan_kernel, gpu/gpu_utils.cuf:90-118, called by
  * gpu_check_nan, gpu/gpu_runner.cuf:5316-5391) extended by cmpdt's

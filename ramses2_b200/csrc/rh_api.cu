@@ -110,7 +110,7 @@ __global__ void unpack_bulk_kernel(double* __restrict__ dst, const float* __rest
 
 // FP64 staging of FP32-bulk uploads / downloads, kept between calls (a host
 // that hands its uold over every step does not pay an allocation each time).
-static int stage64(long long noct, double** out) {
+int stage64(long long noct, double** out) {
   Context& c = ctx();
   const size_t need = sizeof(double) * 40 * (size_t)noct;
   if (c.stage64_bytes < need) {
@@ -248,6 +248,7 @@ static void free_tables(LevelTables& t) {
 
 static void free_state() {
   Context& c = ctx();
+  free_host_schedule();
   for (auto& t : c.levels) free_tables(t);
   c.levels.clear();
   for (int i = 0; i < 2; ++i) {
@@ -853,19 +854,37 @@ int rh_cmpdt(int head_idx, int num_octs, double dx, double gamma, double smallr,
   return RH_OK;
 }
 
+}  // extern "C"
+
+namespace rh {
+
+// Pencil tables of level l for the tile the level's launches use (built, or
+// rebuilt after a tile change, on demand).
+int ensure_level_tables(int l) {
+  Context& c = ctx();
+  LevelTables& T = c.levels[l];
+  const TileCfg& want = c.nlevels_used > 1 ? c.amr_cfg : c.cfg;
+  if (T.complete || !T.built) {
+    if (!T.built || T.cfg.txo != want.txo || T.cfg.tyo != want.tyo || T.cfg.lz != want.lz)
+      return build_level_tables(l, want);
+  }
+  return RH_OK;
+}
+
 // Launch one Godunov step of level l with the given tile configuration.
-// Exposed to the batch/bench layer through rh_godunov and rh_bench_*.
-static int launch_level(int l, double gamma, double smallr, double smallc, double dt, double dx, double smax_cap,
-                        int slope, int riemann, const double* g, bool fuse_cfl, bool accumulate = false) {
+// Exposed to the batch/bench layer through rh_godunov and rh_bench_*.  With
+// `range` only the pencils it lists run (its headers, table offsets and CFL
+// partial slots; no partial reduction): rh_coarse_step_host launches a level
+// group by group that way.
+int launch_level(int l, double gamma, double smallr, double smallc, double dt, double dx, double smax_cap,
+                 int slope, int riemann, const double* g, bool fuse_cfl, bool accumulate, const PencilRange* range) {
   Context& c = ctx();
   LevelTables& T = c.levels[l];
   const bool amr = c.nlevels_used > 1;  // refined cells / coarse-fine faces exist on every level
   const TileCfg& want = amr ? c.amr_cfg : c.cfg;
-  if (T.complete || !T.built) {
-    if (!T.built || T.cfg.txo != want.txo || T.cfg.tyo != want.tyo || T.cfg.lz != want.lz) {
-      int rc = build_level_tables(l, want);
-      if (rc) return rc;
-    }
+  {
+    int rc = ensure_level_tables(l);
+    if (rc) return rc;
   }
   size_t smem = 0;
   int threads = 0;
@@ -881,11 +900,13 @@ static int launch_level(int l, double gamma, double smallr, double smallc, doubl
     if (rc) return rc;
   }
   if (T.npencil == 0) return RH_OK;
+  if (range && range->n == 0) return RH_OK;
   LevelArgs A;
-  A.phdr = T.d_phdr;
-  A.poff = T.d_poff;
-  A.ptab = T.d_ptab;
-  A.npencil = T.npencil;
+  A.phdr = range ? range->phdr : T.d_phdr;
+  A.poff = range ? range->poff : T.d_poff;
+  A.ptab = range ? range->ptab : T.d_ptab;
+  A.npencil = range ? range->n : T.npencil;
+  const int nblocks = A.npencil;
   A.ncx = 2 * T.nxo;
   A.ncy = 2 * T.nyo;
   A.ncz = 2 * T.nzo;
@@ -897,7 +918,7 @@ static int launch_level(int l, double gamma, double smallr, double smallc, doubl
   const double courant = lkey[4] > 0 ? lkey[4] : smax_cap * dt / dx;
   A.cfl = make_cfl(dx, gamma, smallr, smallc, courant, g);
   A.vol = dx * dx * dx;
-  A.cfl_partial = fuse_cfl ? T.d_cfl_partial : nullptr;
+  A.cfl_partial = fuse_cfl ? (range ? range->partial : T.d_cfl_partial) : nullptr;
   A.refmask = c.d_refmask;
   A.ghost_father = c.d_gfather;
   A.accumulate = accumulate ? 1 : 0;
@@ -916,7 +937,7 @@ static int launch_level(int l, double gamma, double smallr, double smallc, doubl
     H.zero = 0.0; H.half = 0.5; H.two = 2.0;
     H.gm1 = gamma - 1.0; H.smalle = A.smalle_d;
     for (int d = 0; d < 3; ++d) H.grav[d] = gh[d];
-    RH_CUDA(fn(A, &S, &H, T.npencil, c.stream));
+    RH_CUDA(fn(A, &S, &H, nblocks, c.stream));
   } else {
     StateArgs<float> S{c.ud[c.cur], c.uf[c.cur], c.ud[nxt], c.uf[nxt]};
     HydroK<float2> H;
@@ -929,14 +950,18 @@ static int launch_level(int l, double gamma, double smallr, double smallc, doubl
     H.zero = b(0.0); H.half = b(0.5); H.two = b(2.0);
     H.gm1 = b(gamma - 1.0); H.smalle = b(A.smalle_d);
     for (int d = 0; d < 3; ++d) H.grav[d] = b(gh[d]);
-    RH_CUDA(fn(A, &S, &H, T.npencil, c.stream));
+    RH_CUDA(fn(A, &S, &H, nblocks, c.stream));
   }
-  if (fuse_cfl) {
+  if (fuse_cfl && !range) {
     reduce_partials_kernel<<<1, 1024, 0, c.stream>>>(T.d_cfl_partial, T.npencil, A.cfl.cdx_smallc, c.d_cfl + 5 * l);
     RH_CUDA(cudaGetLastError());
   }
   return RH_OK;
 }
+
+}  // namespace rh
+
+extern "C" {
 
 int rh_godunov(int head_idx, int num_subgrids, int ngridmax, int ilevel, int levelmin, int levelmax, double gamma,
                double smallr, double smallc2, double dt, double dx, double smax_cap, int slope, int riemann,

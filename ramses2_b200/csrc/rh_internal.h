@@ -122,6 +122,35 @@ int build_complete_tables_device(int l, const TileCfg& cfg, LevelTables& T);
 // device state check of every level (rh_check.cu): RH_EBADSTATE on a bad cell
 int check_all_levels();
 
+// A set of pencils of a level launched on its own (rh_hoststep.cu): device
+// arrays of n pencil headers and table offsets into the oct table ptab (built
+// for the level's tile shape, possibly another pencil depth), and n CFL
+// partial slots.
+struct PencilRange {
+  const int4* phdr;
+  const long long* poff;
+  const int* ptab;
+  double* partial;
+  int n;
+};
+// rh_api.cu: one Godunov step of level l (all pencils, or `range`'s), and the
+// FP64 staging buffer of FP32-bulk transfers (grown on demand, kept).
+int launch_level(int l, double gamma, double smallr, double smallc, double dt, double dx, double smax_cap,
+                 int slope, int riemann, const double* g, bool fuse_cfl, bool accumulate = false,
+                 const PencilRange* range = nullptr);
+int stage64(long long noct, double** out);
+int ensure_level_tables(int l);
+// rh_hoststep.cu: releases the overlapped host-step schedule (mesh change, finalize)
+void free_host_schedule();
+#ifdef __CUDACC__
+__global__ void pack_bulk_kernel(const double* __restrict__ src, float* __restrict__ uf, double* __restrict__ ue,
+                                 long long noct);
+__global__ void unpack_bulk_kernel(double* __restrict__ dst, const float* __restrict__ uf,
+                                   const double* __restrict__ ue, long long noct);
+__global__ void reduce_partials_kernel(const double* __restrict__ partial, long long n, double dt0,
+                                       double* __restrict__ out);
+#endif
+
 // restart / snapshot file images (rh_io.cu)
 struct ImageSrc {
   const double* ud = nullptr;  // FP64: [oct][5][8]; FP32-bulk: the records' E view (rh_bulk.h)

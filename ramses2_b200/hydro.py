@@ -135,6 +135,20 @@ class GodunovGPU:
         check(self.L.rh_coarse_step(C.byref(self.params), C.byref(d), None), "rh_coarse_step")
         return d.value
 
+    def coarse_step_host(self, host_in, host_out=None, dt=None):
+        """rh_coarse_step_host: one coarse step of a state held on the host
+        (host_in, the reference layout; written to host_out, default host_in),
+        the copies overlapped with the pencils.  Returns (dt taken, dt_next)."""
+        host_out = host_in if host_out is None else host_out
+        for a in (host_in, host_out):
+            assert a.dtype == np.float64 and a.flags.c_contiguous and a.shape == self.mesh.uold.shape
+        d = C.c_double(0.0 if dt is None else float(dt))
+        nxt = C.c_double()
+        check(self.L.rh_coarse_step_host(C.byref(self.params), C.c_void_p(host_in.ctypes.data),
+                                         C.c_void_p(host_out.ctypes.data), C.byref(d), C.byref(nxt)),
+              "rh_coarse_step_host")
+        return d.value, nxt.value
+
     # ---- restart / snapshot files (include/ramses_hydro_io.h) -------------------
     def file_image(self, kind):
         """Bytes of the amr / hydro_backup / hydro_output file of the current state."""
