@@ -55,6 +55,18 @@ int rh_level_ghosts(int ilevel, int* gsrc_oct, unsigned char* gsrc_cf, int* gfat
  * step would have changed. */
 int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl);
 
+/* Coarse-fine update of the father cells (unew of level l-1 += or -= the
+ * flux/8 of every face between a cell of level l and an interpolated ghost,
+ * hydro/godunov_fine.f90:893-1052).  0 (the default): atomic FP64 adds from
+ * the pencil kernels, whose order between pencils varies from run to run.
+ * 1: each face's contribution goes to its own slot and one thread per father
+ * cell adds its 24 slots in a fixed order after the level's kernel (the role
+ * of the reference's fixed-order flush of cache octs, godunov_fine.f90:
+ * 1347-1459), so FP64 AMR runs repeat bit for bit; it costs a zeroed buffer of
+ * 960 bytes per ghost oct and one more small kernel per level step.  FP64
+ * precision mode only (FP32-bulk keeps the atomic adds). */
+int rh_set_deterministic(int on);
+
 /* One coarse step of a mesh whose uold lives in host memory: host_in (the
  * reference layout uold(1:8,1:5,1:ngridmax)) is copied to the device, stepped
  * as rh_coarse_step steps it, and the new state is written to host_out (may

@@ -43,6 +43,7 @@ SIGNATURES = {
     "rh_level_table": (_i, [_i, _P(_i), _P(C.c_longlong), _P(_i), C.c_longlong]),
     "rh_level_ghosts": (_i, [_i, _P(_i), _P(C.c_ubyte), _P(_i), C.c_longlong]),
     "rh_set_table_builder": (_i, [_i]),
+    "rh_set_deterministic": (_i, [_i]),
     "rh_coarse_step": (_i, [_P(HydroParams), _P(_d), _P(_d)]),
     "rh_coarse_step_host": (_i, [_P(HydroParams), C.c_void_p, C.c_void_p, _P(_d), _P(_d)]),
     "rh_state_ptrs": (_i, [_P(C.c_void_p), _P(C.c_void_p), _P(C.c_void_p), _P(C.c_void_p)]),

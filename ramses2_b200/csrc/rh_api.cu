@@ -389,6 +389,7 @@ int rh_finalize(void) {
   free_state();
   cudaFree(c.d_err);
   cudaFree(c.d_check);
+  cudaFree(c.d_gface);
   cudaFreeHost(c.h_cfl);
   cudaEventDestroy(c.ev0);
   cudaEventDestroy(c.ev1);
@@ -858,6 +859,26 @@ int rh_cmpdt(int head_idx, int num_octs, double dx, double gamma, double smallr,
 
 namespace rh {
 
+// The deterministic coarse-fine update: each ghost oct of the level adds the
+// 24 face slots its neighbours' pencils stored (zero where no real cell
+// borders it) to its father cell, in slot order, one thread per (ghost, var):
+// the sums no longer depend on which pencil ran first.  The role of the
+// reference's fixed-order flush of cache octs (hydro/godunov_fine.f90:
+// 1347-1459) for the father cells of a level.
+__global__ void coarse_gather_kernel(const double* __restrict__ gface, int nghost, const int2* __restrict__ fathers,
+                                     double* __restrict__ unew) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nghost * 5) return;
+  const int g = (int)(i / 5), v = (int)(i % 5);
+  const int2 fa = fathers[g];
+  if (fa.x < 0) return;
+  const double* s = gface + (size_t)g * 24 * 5 + v;
+  double sum = 0.0;
+#pragma unroll 4
+  for (int f = 0; f < 24; ++f) sum += s[5 * f];
+  unew[(size_t)fa.x * 40 + 8 * v + fa.y] += sum;
+}
+
 // Pencil tables of level l for the tile the level's launches use (built, or
 // rebuilt after a tile change, on demand).
 int ensure_level_tables(int l) {
@@ -922,6 +943,22 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
   A.refmask = c.d_refmask;
   A.ghost_father = c.d_gfather;
   A.accumulate = accumulate ? 1 : 0;
+  A.gface = nullptr;
+  A.gface_base = T.gbase;
+  const bool gather = amr && c.deterministic && c.precision == RH_PREC_FP64 && T.nghost > 0;
+  if (gather) {
+    const size_t need = (size_t)T.nghost * 24 * 5;
+    if (c.gface_elems < need) {
+      RH_CUDA(cudaStreamSynchronize(c.stream));
+      cudaFree(c.d_gface);
+      c.d_gface = nullptr;
+      c.gface_elems = 0;
+      RH_CUDA(cudaMalloc(&c.d_gface, sizeof(double) * need));
+      c.gface_elems = need;
+    }
+    RH_CUDA(cudaMemsetAsync(c.d_gface, 0, sizeof(double) * need, c.stream));
+    A.gface = c.d_gface;
+  }
   const int nxt = 1 - c.cur;
   A.gm1_d = gamma - 1.0;
   A.smalle_d = smallc * smallc / gamma / (gamma - 1.0);
@@ -951,6 +988,11 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
     H.gm1 = b(gamma - 1.0); H.smalle = b(A.smalle_d);
     for (int d = 0; d < 3; ++d) H.grav[d] = b(gh[d]);
     RH_CUDA(fn(A, &S, &H, nblocks, c.stream));
+  }
+  if (gather) {
+    coarse_gather_kernel<<<(unsigned)((T.nghost * 5ll + 255) / 256), 256, 0, c.stream>>>(
+        c.d_gface, T.nghost, c.d_gfather + (T.gbase - c.ngridmax), c.ud[nxt]);
+    RH_CUDA(cudaGetLastError());
   }
   if (fuse_cfl && !range) {
     reduce_partials_kernel<<<1, 1024, 0, c.stream>>>(T.d_cfl_partial, T.npencil, A.cfl.cdx_smallc, c.d_cfl + 5 * l);
@@ -1227,6 +1269,13 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
   }
   *dt = step_dt;
   if (c.state_check) return check_all_levels();  // the reference's gpu_debug scan after set_uold
+  return RH_OK;
+}
+
+int rh_set_deterministic(int on) {
+  int rc = check_ready(false);
+  if (rc) return rc;
+  ctx().deterministic = on ? 1 : 0;
   return RH_OK;
 }
 

@@ -130,6 +130,11 @@ struct LevelArgs {
   const uint8_t* refmask;  // per oct (real and ghost): bit c = cell c refined
   const int2* ghost_father;  // per ghost (entry - ghost_base): father oct (0-based), father cell
   int accumulate;          // 1: unew already holds uold (+ finer-level corrections); add to it
+  // deterministic coarse-fine update (FP64): per ghost oct of this level 24
+  // face slots (ghost cell x direction) of 5 values, summed later in a fixed
+  // order by coarse_gather_kernel; null: atomic adds into the fathers
+  double* gface;
+  long long gface_base;    // state entry of the level's first ghost oct
 };
 
 // Coarse-fine status of one cell of an AMR level (hydro/godunov_fine.f90:
@@ -147,9 +152,19 @@ __device__ __forceinline__ uint32_t amr_bits(const LevelArgs& A, int ent, int ce
 }
 
 // Flux through the face between a cell of this level and an interpolated
-// ghost: unew(father) +- flux/8 (sign -1: ghost on the low side).
+// ghost: unew(father) +- flux/8 (sign -1: ghost on the low side).  slot =
+// 3 * (ghost cell in its oct) + direction names the face: a ghost cell has one
+// face per direction on its oct's boundary, and only the pencil holding the
+// real cell across it writes there.  Atomic adds into the father, or (A.gface
+// set) a store into the face's slot for coarse_gather_kernel.
 __device__ __forceinline__ void coarse_add_f64(const LevelArgs& A, double* unew, int ghost_ent, const double* f,
-                                               double sign) {
+                                               double sign, int slot) {
+  if (A.gface) {
+    double* s = A.gface + ((size_t)(ghost_ent - A.gface_base) * 24 + slot) * 5;
+#pragma unroll
+    for (int n = 0; n < 5; ++n) s[n] = sign * (f[n] * 0.125);
+    return;
+  }
   const int2 fa = A.ghost_father[ghost_ent - A.ghost_base];
   if (fa.x < 0) return;
   double* o = unew + (size_t)fa.x * 40 + fa.y;

@@ -59,6 +59,9 @@ struct Context {
   bool amr_cfg_set = false;     // amr_cfg chosen by rh_set_amr_tile (else by precision at rh_set_mesh)
   int table_builder = 1;        // coarse-fine tables: 1 on the device, 0 on the host
   int state_check = 0;          // rh_coarse_step checks every level after set_uold (rh_set_state_check)
+  int deterministic = 0;        // FP64 coarse-fine update through face slots (rh_set_deterministic)
+  double* d_gface = nullptr;    // [ghost octs of a level][24 faces][5] slots of that update
+  size_t gface_elems = 0;
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;

@@ -21,7 +21,8 @@ PRECISION = {"fp64": RH_PREC_FP64, "fp32_bulk": RH_PREC_FP32_BULK, "fp32": RH_PR
 class GodunovGPU:
     """One mesh resident on one B200, stepped through the C ABI."""
 
-    def __init__(self, mesh, params, precision="fp64", device=0, tile=None, amr_tile=None, table_builder=None):
+    def __init__(self, mesh, params, precision="fp64", device=0, tile=None, amr_tile=None, table_builder=None,
+                 deterministic=False):
         self.mesh = mesh
         self.params = params
         self.L = lib()
@@ -36,6 +37,7 @@ class GodunovGPU:
         if table_builder is not None:
             check(self.L.rh_set_table_builder({"host": 0, "device": 1}.get(table_builder, table_builder)),
                   "rh_set_table_builder")
+        check(self.L.rh_set_deterministic(int(bool(deterministic))), "rh_set_deterministic")
         self._desc = mesh.desc()
         check(self.L.rh_set_mesh(C.byref(self._desc), dptr(mesh.uold), 5, 8), "rh_set_mesh")
         g = np.ascontiguousarray(mesh.gravity, np.float64)

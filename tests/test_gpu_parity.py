@@ -387,6 +387,35 @@ def test_config1_form_amr_independent_runs_24_steps(prec):
         gpu.close()
 
 
+def test_amr_deterministic_coarse_update_repeats_bitwise():
+    """rh_set_deterministic(1): the FP64 coarse-fine corrections go through
+    per-face slots summed in a fixed order, so two AMR runs of four coarse
+    steps are bitwise equal, and each stays within 1e-12 of the oracle."""
+    m, P = amr_case("outflow", 1, 0)
+    u0 = m.uold.copy()
+    o = oracle.OracleHydro(m, P, nthreads=NTHREADS)
+    refs = []
+    for _ in range(4):
+        amr_step(o, m)
+        refs.append(m.uold.copy())
+    runs = []
+    for _ in range(2):
+        m.uold[:] = u0
+        gpu = GodunovGPU(m, P, precision="fp64", deterministic=True)
+        try:
+            states = []
+            for s in range(4):
+                gpu.coarse_step()
+                states.append(gpu.fetch_uold())
+                err = rel_l1(states[-1], refs[s])
+                assert np.all(err <= TOL_FP64), (s, err)
+        finally:
+            gpu.close()
+        runs.append(states)
+    for a, b in zip(*runs):
+        assert np.array_equal(a, b)
+
+
 def test_amr_coarse_step_native_given_dt_fp32_bulk():
     """rh_coarse_step with the oracle's dt passed in (no courant_fine):
     FP32-bulk density within 1e-5 of the oracle's coarse step."""
