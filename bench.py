@@ -284,12 +284,32 @@ def bench_serve(args, rank, world, dist):
         if dist is not None:
             dist.barrier()
         sb = srv.run(burst, realtime=False)
-        srv.close()
+        local_rate = sb["cell_updates_per_s"]  # this GPU's capacity (each rank serves its own stream)
         if dist is not None:
             sb["cell_updates"] = sum_over_ranks([sb["cell_updates"]], dist)[0]
             sb["makespan_s"] = max_over_ranks([sb["makespan_s"]], dist)[0]
             sb["cell_updates_per_s"] = sb["cell_updates"] / sb["makespan_s"]
         st["burst"] = {k: sb[k] for k in ("makespan_s", "cell_updates_per_s", "latency_p50_s", "latency_p99_s")}
+        # latency against offered load: Poisson streams at fractions of the
+        # burst capacity (requests/s = burst cell-updates/s over the mean
+        # cell-updates of a request of this mix)
+        if args.serve_sweep_requests > 0:
+            probe = make_requests(args.serve_sweep_requests, rate_hz=1.0, seed=777 + rank)
+            mean_work = float(np.mean([r.solved_cells * r.target_steps for r in probe]))
+            cap_rps = local_rate / mean_work
+            sweep = []
+            for frac in (0.25, 0.5, 0.8, 0.95):
+                reqs = make_requests(args.serve_sweep_requests, rate_hz=frac * cap_rps, seed=777 + rank)
+                if dist is not None:
+                    dist.barrier()
+                sp = srv.run(reqs, realtime=True)
+                sweep.append({"offered_load_of_burst": frac, "rate_hz": frac * cap_rps,
+                              "latency_p50_s": sp["latency_p50_s"], "latency_p99_s": sp["latency_p99_s"],
+                              "cell_updates_per_s": sp["cell_updates_per_s"], "makespan_s": sp["makespan_s"],
+                              "requests": sp["requests"]})
+            st["load_sweep"] = {"capacity_requests_per_s": cap_rps, "mean_cell_updates_per_request": mean_work,
+                                "points": sweep}
+        srv.close()
         if dist is not None:
             st["cell_updates"] = sum_over_ranks([st["cell_updates"]], dist)[0]
             st["makespan_s"] = max_over_ranks([st["makespan_s"]], dist)[0]
@@ -898,6 +918,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=50)
     ap.add_argument("--serve-requests", type=int, default=60, help="serving session length (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="request arrivals per second")
+    ap.add_argument("--serve-sweep-requests", type=int, default=100,
+                    help="requests per point of the latency-vs-offered-load sweep (0: skip)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

@@ -66,6 +66,32 @@ template <class V> __device__ __forceinline__ V momentum_bound(V dq, V rm1, V vm
   return vcopysign(vmin(vabs(dq), dlim), dq);
 }
 
+
+// Half of limited_slope and of the momentum bound (FP64 lanes), for slope
+// types 1 and 2: bitwise 0.5 * the full values (scaling by two commutes with
+// rounding, so 0.5 * (2 min) = min and 0.5 * (0.5 (a + b)) = 0.25 (a + b)
+// exactly).  The FP64 body takes these: two multiplications fewer per slope,
+// and its registers fit without spilling (the FP32-bulk body ran 2 % slower
+// with them and keeps the full slopes times one half).
+template <int SLOPE> __device__ __forceinline__ double half_slope(double qm1, double q0, double qp1) {
+  if (SLOPE == 0) return 0.0;
+  const double a = q0 - qm1, b = qp1 - q0;
+  if (SLOPE == 1) {
+    const double r = vsel(vgt(a, 0.0), vmin(a, b), vmax(a, b));
+    return 0.5 * vsel(vgt(a * b, 0.0), r, 0.0);
+  }
+  const double dcen = 0.25 * (a + b);
+  const double dlim = vsel(vgt(a * b, 0.0), vmin(vabs(a), vabs(b)), 0.0);
+  return vcopysign(vmin(dlim, vabs(dcen)), dcen);
+}
+__device__ __forceinline__ double half_momentum_bound(double dq, double rm1, double vm1, double v0, double rp1,
+                                                      double vp1, double ir0) {
+  const double dlft = rm1 * vabs(v0 - vm1);
+  const double drgt = rp1 * vabs(vp1 - v0);
+  const double dlim = vmin(dlft, drgt) * ir0;
+  return vcopysign(vmin(vabs(dq), dlim), dq);
+}
+
 // HLLC (Toro), godunov_utils.f90:638-852.  q = (rho, un, ut1, ut2, p);
 // f = (mass, normal momentum, t1 momentum, t2 momentum, total energy).
 template <class V> __device__ __forceinline__ void riemann_hllc(const V* ql, const V* qr, V* f, const HydroK<V>& H) {
