@@ -284,19 +284,20 @@ def bench_serve(args, rank, world, dist):
         if dist is not None:
             dist.barrier()
         sb = srv.run(burst, realtime=False)
-        local_rate = sb["cell_updates_per_s"]  # this GPU's capacity (each rank serves its own stream)
         if dist is not None:
             sb["cell_updates"] = sum_over_ranks([sb["cell_updates"]], dist)[0]
             sb["makespan_s"] = max_over_ranks([sb["makespan_s"]], dist)[0]
             sb["cell_updates_per_s"] = sb["cell_updates"] / sb["makespan_s"]
         st["burst"] = {k: sb[k] for k in ("makespan_s", "cell_updates_per_s", "latency_p50_s", "latency_p99_s")}
-        # latency against offered load: Poisson streams at fractions of the
-        # burst capacity (requests/s = burst cell-updates/s over the mean
-        # cell-updates of a request of this mix)
+        # latency against offered load: the sweep's request set (its problems
+        # do not depend on the rate) served as a burst gives this GPU's
+        # capacity in requests/s; Poisson streams of it then arrive at
+        # fractions of that capacity
         if args.serve_sweep_requests > 0:
             probe = make_requests(args.serve_sweep_requests, rate_hz=1.0, seed=777 + rank)
-            mean_work = float(np.mean([r.solved_cells * r.target_steps for r in probe]))
-            cap_rps = local_rate / mean_work
+            pb = srv.run(probe, realtime=False)
+            mean_work = pb["cell_updates"] / max(1, pb["served"])
+            cap_rps = pb["served"] / pb["makespan_s"]
             sweep = []
             for frac in (0.25, 0.5, 0.8, 0.95):
                 reqs = make_requests(args.serve_sweep_requests, rate_hz=frac * cap_rps, seed=777 + rank)
@@ -308,7 +309,7 @@ def bench_serve(args, rank, world, dist):
                               "cell_updates_per_s": sp["cell_updates_per_s"], "makespan_s": sp["makespan_s"],
                               "requests": sp["requests"]})
             st["load_sweep"] = {"capacity_requests_per_s": cap_rps, "mean_cell_updates_per_request": mean_work,
-                                "points": sweep}
+                                "burst_cell_updates_per_s": pb["cell_updates_per_s"], "points": sweep}
         srv.close()
         if dist is not None:
             st["cell_updates"] = sum_over_ranks([st["cell_updates"]], dist)[0]
@@ -389,7 +390,7 @@ def leaf_rel_l1(m, a, b):
 
 
 def bench_amr(args, rank, world, dist, device):
-    """Config 1: AMR Sedov on levels 7-10 refined by hydro_refine's 0.1
+    """AMR Sedov on levels 7-10 refined by hydro_refine's 0.1
     density/pressure gradient criterion on a developed Sedov-like blast
     (2-6 M leaf cells), HLLC, moncen, Courant 0.8, args.amr_steps coarse
     steps with nsubcycle=1 (courant_fine of every level, then every level's
@@ -569,7 +570,7 @@ def bench_sedov512(args, rank, world, dist, device, tuned):
 
 
 def bench_turbulence(args, rank, world, dist, device):
-    """Config-2: decaying supersonic turbulence on 256^3 (gamma 1.001, rms
+    """Decaying supersonic turbulence on 256^3 (gamma 1.001, rms
     Mach 5, lognormal density, minmod, HLLC, periodic), tiles autotuned on
     this state, args.turb_steps FP32-bulk and FP64 steps; FP32-bulk relative
     L1 against FP64 after them."""
@@ -745,7 +746,7 @@ def run_ours(args):
         cpu = {"value": ncell / cpu_s, "unit": "cell-updates/s", "cores": nthreads, "kind": "port",
                "sample": "one full 256^3 Sedov step (courant_fine + godunov_fine, OpenMP over oct blocks "
                          "on %d threads) of the CPU restatement of the reference path, %.2f s" % (nthreads, cpu_s)}
-        # the config-0 size (Sedov 64^3) on one thread and on all of them, a few steps each
+        # Sedov 64^3 (outflow, 100-step size) on one thread and on all of them, a few steps each
         from ramses2_b200.mesh import sedov3d, uniform_mesh
 
         c0 = {}

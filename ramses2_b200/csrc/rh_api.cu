@@ -481,7 +481,7 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
   int rc = check_ready(false);
   if (rc) return rc;
   Context& c = ctx();
-  // coarse-fine tile unless chosen: the fastest on config 1's AMR Sedov per precision
+  // coarse-fine tile unless chosen: the fastest on the AMR Sedov of levels 7-10 per precision
   if (!c.amr_cfg_set) c.amr_cfg = c.precision == RH_PREC_FP32_BULK ? TileCfg{7, 7, 2, 8} : TileCfg{8, 4, 2, 8};
   if (!m || !uold || !m->grid || !m->head || !m->noct) {
     set_error("rh_set_mesh: null pointer");
@@ -628,7 +628,7 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
       if (rc) return rc;
       continue;
     }
-    rc = build_level_tables(l, multi ? c.amr_cfg : c.cfg);
+    rc = build_level_tables(l, level_cfg(l));
     if (rc) {
       // keep the mesh usable for set_unew/set_uold/cmpdt; godunov on this
       // level will report the table error
@@ -879,12 +879,25 @@ __global__ void coarse_gather_kernel(const double* __restrict__ gface, int nghos
   unew[(size_t)fa.x * 40 + 8 * v + fa.y] += sum;
 }
 
+// Tile of level l's launches: the uniform tile on a single-level mesh, the
+// coarse-fine tile (kernels that handle refined cells and interpolated ghosts)
+// on every level of a multi-level mesh.  (A level that fills its box could
+// take deeper pencils, with fewer halo layers per cell; on the AMR Sedov of
+// levels 7-10, 32 layers on its complete level 7 made the FP32-bulk coarse
+// step slower, 0.771 -> 0.825 ms, and the FP64 one 1.4 % faster, so every
+// level keeps the coarse-fine tile.)
+TileCfg level_cfg(int l) {
+  Context& c = ctx();
+  (void)l;
+  return c.nlevels_used > 1 ? c.amr_cfg : c.cfg;
+}
+
 // Pencil tables of level l for the tile the level's launches use (built, or
 // rebuilt after a tile change, on demand).
 int ensure_level_tables(int l) {
   Context& c = ctx();
   LevelTables& T = c.levels[l];
-  const TileCfg& want = c.nlevels_used > 1 ? c.amr_cfg : c.cfg;
+  const TileCfg want = level_cfg(l);
   if (T.complete || !T.built) {
     if (!T.built || T.cfg.txo != want.txo || T.cfg.tyo != want.tyo || T.cfg.lz != want.lz)
       return build_level_tables(l, want);
@@ -902,7 +915,7 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
   Context& c = ctx();
   LevelTables& T = c.levels[l];
   const bool amr = c.nlevels_used > 1;  // refined cells / coarse-fine faces exist on every level
-  const TileCfg& want = amr ? c.amr_cfg : c.cfg;
+  const TileCfg want = level_cfg(l);
   {
     int rc = ensure_level_tables(l);
     if (rc) return rc;

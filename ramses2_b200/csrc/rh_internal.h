@@ -143,6 +143,7 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
                  const PencilRange* range = nullptr);
 int stage64(long long noct, double** out);
 int ensure_level_tables(int l);
+TileCfg level_cfg(int l);  // tile of level l's launches (see rh_api.cu)
 // rh_hoststep.cu: releases the overlapped host-step schedule (mesh change, finalize)
 void free_host_schedule();
 #ifdef __CUDACC__

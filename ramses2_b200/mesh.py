@@ -400,7 +400,7 @@ def fill_amr_prim(mesh, prim_fn, gamma):
 
 
 # ---------------------------------------------------------------------------
-# Gradient refinement criterion and a developed Sedov-like blast (config 1)
+# Gradient refinement criterion and a developed Sedov-like blast (the AMR Sedov mesh)
 # ---------------------------------------------------------------------------
 def hydro_refine_flags(prim_fn, x, dx, err_grad_d=0.1, err_grad_p=0.1, floor_d=1e-10, floor_p=1e-10):
     """hydro_refine's density and pressure criteria (hydro/godunov_utils.f90:
@@ -450,7 +450,7 @@ def sedov_like_blast(radius=0.2, gamma=1.4, energy=1.0, rho0=1.0, p0=1e-5, centr
 
 
 def sedov_amr_mesh(levelmin=7, levelmax=10, radius=0.2, gamma=1.4, err_grad=0.1, bc="outflow"):
-    """Config-1 style mesh: levels levelmin..levelmax refined where
+    """AMR Sedov mesh: levels levelmin..levelmax refined where
     hydro_refine's relative density/pressure gradient exceeds ``err_grad`` on
     a developed Sedov-like blast (:func:`sedov_like_blast`), filled with that
     state.  Returns (mesh, gamma)."""

@@ -74,7 +74,7 @@ def test_device_tables_equal_host_tables(name, amr_tile):
     assert nghost > 0
 
 
-def test_device_tables_on_config1_mesh():
+def test_device_tables_on_amr_sedov_mesh():
     m, _ = sedov_amr_mesh(6, 8, radius=0.15)
     host = tables(m, "host", (8, 4, 2, 8))
     dev = tables(m, "device", (8, 4, 2, 8))

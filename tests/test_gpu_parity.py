@@ -128,7 +128,7 @@ def test_courant_fine_parity():
 
 
 def test_sedov_multistep_fp64():
-    """Config-0 style Sedov (moncen, HLLC, C=0.8, outflow) at 32^3: both paths
+    """Sedov (moncen, HLLC, C=0.8, outflow) at 32^3: both paths
     evolve independently for 12 steps; every step stays within the bar and
     the fused CFL values match the oracle's courant_fine."""
     m = uniform_mesh(5, nsubgrid=1, bc="outflow")
@@ -150,8 +150,8 @@ def test_sedov_multistep_fp64():
         gpu.close()
 
 
-def test_config0_sedov64_per_step_over_100_steps():
-    """Config 0 as specified: Sedov 64^3 (levelmin = levelmax = 6, outflow,
+def test_sedov64_per_step_over_100_steps():
+    """Sedov 64^3 (levelmin = levelmax = 6, outflow,
     gamma 1.4, E = 1 within 2 cells, moncen, HLLC, C = 0.8), 100 steps.  Each
     step the GPU starts from the oracle's state (rh_set_grid_device) and takes
     the oracle's dt: relative L1 <= 1e-12 per variable at every step.  The
@@ -350,8 +350,8 @@ def test_amr_coarse_step_native(bc, itype, ivar, spare):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32_bulk"])
-def test_config1_form_amr_independent_runs_24_steps(prec):
-    """Config 1's form on a small mesh: Sedov on levels 3-5 refined by
+def test_amr_sedov_levels3to5_independent_runs_24_steps(prec):
+    """The AMR Sedov on a small mesh: levels 3-5 refined by
     hydro_refine's 0.1 gradient criteria (outflow, gamma 1.4, moncen, HLLC,
     C = 0.8, interpol_type 1), 24 coarse steps with nsubcycle = 1.  The GPU
     (rh_coarse_step, its own courant_fine dt) and the oracle evolve
