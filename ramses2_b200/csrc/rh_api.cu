@@ -987,7 +987,7 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
     H.zero = 0.0; H.half = 0.5; H.two = 2.0;
     H.gm1 = gamma - 1.0; H.smalle = A.smalle_d;
     for (int d = 0; d < 3; ++d) H.grav[d] = gh[d];
-    RH_CUDA(fn(A, &S, &H, nblocks, c.stream));
+    RH_CUDA(fn(A, &S, &H, nblocks, range && range->stream ? range->stream : c.stream));
   } else {
     StateArgs<float> S{c.ud[c.cur], c.uf[c.cur], c.ud[nxt], c.uf[nxt]};
     HydroK<float2> H;
@@ -1000,7 +1000,7 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
     H.zero = b(0.0); H.half = b(0.5); H.two = b(2.0);
     H.gm1 = b(gamma - 1.0); H.smalle = b(A.smalle_d);
     for (int d = 0; d < 3; ++d) H.grav[d] = b(gh[d]);
-    RH_CUDA(fn(A, &S, &H, nblocks, c.stream));
+    RH_CUDA(fn(A, &S, &H, nblocks, range && range->stream ? range->stream : c.stream));
   }
   if (gather) {
     coarse_gather_kernel<<<(unsigned)((T.nghost * 5ll + 255) / 256), 256, 0, c.stream>>>(

@@ -9,6 +9,10 @@
 // chunk they need and each group is launched when that chunk is on the device
 // (FP32-bulk: packed into its oct records).  A chunk is downloaded on a second
 // copy stream once the last group that writes one of its octs has finished.
+// Four streams in all (library, upload, unpack, download): spreading the
+// groups over eight more streams, beyond CUDA's default eight hardware work
+// queues, made the copies queue behind kernels (26.6 ms per 256^3 step
+// against 18.1).
 // The pencil kernel is the one rh_coarse_step runs (the level's tile shape),
 // launched group by group over the schedule's own pencil tables, 8 layers
 // deep.  A cell's update does not depend on where pencils start and end, so
@@ -64,7 +68,12 @@ namespace {
 // the pencils that write it, so shallow pencils start earlier and release
 // chunks sooner; the pencils' extra halo work is hidden behind the copies.
 constexpr int kLz = 8;
-constexpr long long kChunkOcts = 16384;  // 5.2 MB of FP64 state per copy
+// 128 chunks of 16,384 octs (5.2 MB of FP64 state per copy) for a 256^3
+// level: on one box 18.8-18.9 ms per FP32-bulk step, against 18.3-19.6 with
+// 256 chunks and 20-21 with 64 (fewer chunks leave a longer tail of downloads
+// after the last upload; more add per-copy cost on a link already carrying
+// both directions).
+constexpr long long kChunkOcts = 16384;
 constexpr int kMaxChunks = 128;
 
 HostStepSched*& sched_ptr() {
@@ -264,8 +273,7 @@ int rh_coarse_step_host(const rh_hydro_params* p, const double* host_in, double*
   auto chunk_octs = [&](int k) { return std::min(S.C, N - k * S.C); };
   // everything queued before this call is done with the state buffers first
   RH_CUDA(cudaEventRecord(S.ev_start, c.stream));
-  RH_CUDA(cudaStreamWaitEvent(S.up, S.ev_start, 0));
-  RH_CUDA(cudaStreamWaitEvent(S.down, S.ev_start, 0));
+  for (cudaStream_t st : {S.up, S.down, S.unpk}) RH_CUDA(cudaStreamWaitEvent(st, S.ev_start, 0));
   const int cur = c.cur, nxt = 1 - c.cur;
   for (int r = 0; r < K; ++r) {
     const int k = S.up_order[r];
@@ -274,11 +282,17 @@ int rh_coarse_step_host(const rh_hydro_params* p, const double* host_in, double*
     RH_CUDA(cudaMemcpyAsync(dst, host_in + o * 40, sizeof(double) * 40 * n, cudaMemcpyHostToDevice, S.up));
     RH_CUDA(cudaEventRecord(S.ev_up[r], S.up));
   }
-  auto pack = [&](int k) -> int {
-    const long long o = k * S.C, n = chunk_octs(k);
-    pack_bulk_kernel<<<(unsigned)((n * 8 + 255) / 256), 256, 0, c.stream>>>(stage + o * 40, c.uf[cur] + o * kBulkF,
-                                                                          c.ud[cur] + o * kBulkD, n);
-    RH_CUDA(cudaGetLastError());
+  // chunk ready for the pencils (FP32-bulk: packed into oct records), in
+  // upload order on the library stream
+  auto ready = [&](int r) -> int {
+    RH_CUDA(cudaStreamWaitEvent(c.stream, S.ev_up[r], 0));
+    if (bulk) {
+      const int k = S.up_order[r];
+      const long long o = k * S.C, n = chunk_octs(k);
+      pack_bulk_kernel<<<(unsigned)((n * 8 + 255) / 256), 256, 0, c.stream>>>(
+          stage + o * 40, c.uf[cur] + o * kBulkF, c.ud[cur] + o * kBulkD, n);
+      RH_CUDA(cudaGetLastError());
+    }
     return RH_OK;
   };
   // courant_fine keys of the fused CFL epilogue (as rh_cmpdt records them)
@@ -288,10 +302,8 @@ int rh_coarse_step_host(const rh_hydro_params* p, const double* host_in, double*
   const bool given = step_dt > 0;
   if (!given) {
     // no dt from the host: the CFL of the uploaded state after the whole upload
-    for (int r = 0; r < K; ++r) {
-      RH_CUDA(cudaStreamWaitEvent(c.stream, S.ev_up[r], 0));
-      if (bulk && (rc = pack(S.up_order[r]))) return rc;
-    }
+    for (int r = 0; r < K; ++r)
+      if ((rc = ready(r))) return rc;
     c.cfl_on_uold[l] = 0;
     c.cfl_on_unew[l] = 0;
     double m, ek, ei, em;
@@ -301,13 +313,11 @@ int rh_coarse_step_host(const rh_hydro_params* p, const double* host_in, double*
   }
   const double smax_cap = p->courant_factor * dx / step_dt;
   for (int r = 0; r < K; ++r) {
-    if (given) {
-      RH_CUDA(cudaStreamWaitEvent(c.stream, S.ev_up[r], 0));
-      if (bulk && (rc = pack(S.up_order[r]))) return rc;
-    }
+    if (given && (rc = ready(r))) return rc;
     const int n = S.gstart[r + 1] - S.gstart[r];
     if (n > 0) {
-      PencilRange R{S.d_phdr + S.gstart[r], S.d_poff + S.gstart[r], S.T.d_ptab, S.d_partial + 5ll * S.gstart[r], n};
+      PencilRange R{S.d_phdr + S.gstart[r], S.d_poff + S.gstart[r], S.T.d_ptab, S.d_partial + 5ll * S.gstart[r], n,
+                    nullptr};
       if ((rc = launch_level(l, p->gamma, p->smallr, p->smallc, step_dt, dx, smax_cap, p->slope_type, p->riemann, g,
                              true, false, &R)))
         return rc;

@@ -135,6 +135,7 @@ struct PencilRange {
   const int* ptab;
   double* partial;
   int n;
+  cudaStream_t stream;  // stream of the launch (the library stream when null)
 };
 // rh_api.cu: one Godunov step of level l (all pencils, or `range`'s), and the
 // FP64 staging buffer of FP32-bulk transfers (grown on demand, kept).
