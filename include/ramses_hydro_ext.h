@@ -62,9 +62,10 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl);
  * 1: each face's contribution goes to its own slot and one thread per father
  * cell adds its 24 slots in a fixed order after the level's kernel (the role
  * of the reference's fixed-order flush of cache octs, godunov_fine.f90:
- * 1347-1459), so FP64 AMR runs repeat bit for bit; it costs a zeroed buffer of
- * 960 bytes per ghost oct and one more small kernel per level step.  FP64
- * precision mode only (FP32-bulk keeps the atomic adds). */
+ * 1347-1459), so AMR runs repeat bit for bit; it costs a zeroed buffer of
+ * 960 bytes per ghost oct and one more small kernel per level step.  Both
+ * precision modes (FP32-bulk: the slot sums are added to the float records
+ * and the FP64 energy in FP64). */
 int rh_set_deterministic(int on);
 
 /* One coarse step of a mesh whose uold lives in host memory: host_in (the

@@ -316,12 +316,12 @@ __global__ void prolong_kernel(const int* __restrict__ src_oct, const unsigned c
 
 }  // namespace
 
-int prolong_ghosts(int l, double smallr) {
+int prolong_ghosts(int l, double smallr, cudaStream_t st) {
   Context& c = ctx();
   LevelTables& T = c.levels[l];
   if (T.nghost == 0) return RH_OK;
   const int threads = 128;
-  prolong_kernel<<<(T.nghost + threads - 1) / threads, threads, 0, c.stream>>>(
+  prolong_kernel<<<(T.nghost + threads - 1) / threads, threads, 0, st ? st : c.stream>>>(
       T.d_gsrc_oct, T.d_gsrc_cf, T.nghost, T.gbase, c.ud[c.cur], c.uf[c.cur],
       c.precision == RH_PREC_FP32_BULK ? 1 : 0, c.interpol_var, c.interpol_type, smallr);
   RH_CUDA(cudaGetLastError());

@@ -377,6 +377,8 @@ int rh_init(int device_ordinal) {
   RH_CUDA(cudaMemset(c.d_err, 0, sizeof(int)));
   RH_CUDA(cudaEventCreate(&c.ev0));
   RH_CUDA(cudaEventCreate(&c.ev1));
+  RH_CUDA(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+  RH_CUDA(cudaEventCreateWithFlags(&c.ev_side_start, cudaEventDisableTiming));
   c.inited = true;
   return RH_OK;
 }
@@ -393,6 +395,9 @@ int rh_finalize(void) {
   cudaFreeHost(c.h_cfl);
   cudaEventDestroy(c.ev0);
   cudaEventDestroy(c.ev1);
+  for (cudaEvent_t e : c.ev_prolong) cudaEventDestroy(e);
+  cudaEventDestroy(c.ev_side_start);
+  cudaStreamDestroy(c.side);
   cudaStreamDestroy(c.stream);
   c = Context();
   return RH_OK;
@@ -892,6 +897,28 @@ TileCfg level_cfg(int l) {
   return c.nlevels_used > 1 ? c.amr_cfg : c.cfg;
 }
 
+// The same for FP32-bulk records: the four float variables and the FP64
+// energy of each father cell receive their slot sums (added up in FP64).
+__global__ void coarse_gather_f32_kernel(const double* __restrict__ gface, int nghost,
+                                         const int2* __restrict__ fathers, float* __restrict__ unew_f,
+                                         double* __restrict__ unew_e) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nghost * 5) return;
+  const int g = (int)(i / 5), v = (int)(i % 5);
+  const int2 fa = fathers[g];
+  if (fa.x < 0) return;
+  const double* s = gface + (size_t)g * 24 * 5 + v;
+  double sum = 0.0;
+#pragma unroll 4
+  for (int f = 0; f < 24; ++f) sum += s[5 * f];
+  if (v < 4) {
+    float* o = unew_f + (size_t)fa.x * kBulkF + 8 * v + fa.y;
+    *o = (float)((double)*o + sum);
+  } else {
+    unew_e[(size_t)fa.x * kBulkD + fa.y] += sum;
+  }
+}
+
 // Pencil tables of level l for the tile the level's launches use (built, or
 // rebuilt after a tile change, on demand).
 int ensure_level_tables(int l) {
@@ -930,8 +957,14 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
     return RH_EINVAL;
   }
   if (amr) {
-    int rc = prolong_ghosts(l, smallr);
-    if (rc) return rc;
+    if (l < (int)c.prolonged.size() && c.prolonged[l]) {
+      // prolonged ahead on the side stream by rh_coarse_step
+      RH_CUDA(cudaStreamWaitEvent(c.stream, c.ev_prolong[l], 0));
+      c.prolonged[l] = 0;
+    } else {
+      int rc = prolong_ghosts(l, smallr);
+      if (rc) return rc;
+    }
   }
   if (T.npencil == 0) return RH_OK;
   if (range && range->n == 0) return RH_OK;
@@ -958,7 +991,7 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
   A.accumulate = accumulate ? 1 : 0;
   A.gface = nullptr;
   A.gface_base = T.gbase;
-  const bool gather = amr && c.deterministic && c.precision == RH_PREC_FP64 && T.nghost > 0;
+  const bool gather = amr && c.deterministic && T.nghost > 0;
   if (gather) {
     const size_t need = (size_t)T.nghost * 24 * 5;
     if (c.gface_elems < need) {
@@ -1003,8 +1036,13 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
     RH_CUDA(fn(A, &S, &H, nblocks, range && range->stream ? range->stream : c.stream));
   }
   if (gather) {
-    coarse_gather_kernel<<<(unsigned)((T.nghost * 5ll + 255) / 256), 256, 0, c.stream>>>(
-        c.d_gface, T.nghost, c.d_gfather + (T.gbase - c.ngridmax), c.ud[nxt]);
+    const unsigned nb = (unsigned)((T.nghost * 5ll + 255) / 256);
+    if (c.precision == RH_PREC_FP64)
+      coarse_gather_kernel<<<nb, 256, 0, c.stream>>>(c.d_gface, T.nghost, c.d_gfather + (T.gbase - c.ngridmax),
+                                                     c.ud[nxt]);
+    else
+      coarse_gather_f32_kernel<<<nb, 256, 0, c.stream>>>(c.d_gface, T.nghost, c.d_gfather + (T.gbase - c.ngridmax),
+                                                         c.uf[nxt], c.ud[nxt]);
     RH_CUDA(cudaGetLastError());
   }
   if (fuse_cfl && !range) {
@@ -1223,6 +1261,34 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
         o[4] = ldt;
       }
       step_dt = std::min(step_dt, ldt);
+    }
+  }
+  // Every level's interpolated ghost octs, prolonged ahead on the side stream:
+  // a level's ghosts come from the coarser level's uold, which no Godunov step
+  // of this coarse step changes before that level's own step (set_uold and
+  // the restrictions of level l-1 follow level l's step), so they overlap the
+  // set_unew copy and the finer levels' steps.
+  // whatever happens below, no level is left marked as prolonged ahead
+  struct ClearProlonged {
+    ~ClearProlonged() { std::fill(ctx().prolonged.begin(), ctx().prolonged.end(), 0); }
+  } clear_prolonged;
+  if (lev.size() > 1) {
+    if (c.ev_prolong.size() < (size_t)(c.levelmax + 1)) {
+      for (size_t k = c.ev_prolong.size(); k < (size_t)(c.levelmax + 1); ++k) {
+        cudaEvent_t e;
+        RH_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c.ev_prolong.push_back(e);
+      }
+    }
+    c.prolonged.assign(c.levelmax + 1, 0);
+    RH_CUDA(cudaEventRecord(c.ev_side_start, c.stream));
+    RH_CUDA(cudaStreamWaitEvent(c.side, c.ev_side_start, 0));
+    for (size_t i = lev.size(); i-- > 0;) {
+      const int l = lev[i];
+      if (!c.levels[l].built || c.levels[l].nghost == 0) continue;
+      if ((rc = prolong_ghosts(l, p->smallr, c.side))) return rc;
+      RH_CUDA(cudaEventRecord(c.ev_prolong[l], c.side));
+      c.prolonged[l] = 1;
     }
   }
   // several levels that together hold every oct of the state: set_unew as

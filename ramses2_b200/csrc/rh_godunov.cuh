@@ -130,9 +130,9 @@ struct LevelArgs {
   const uint8_t* refmask;  // per oct (real and ghost): bit c = cell c refined
   const int2* ghost_father;  // per ghost (entry - ghost_base): father oct (0-based), father cell
   int accumulate;          // 1: unew already holds uold (+ finer-level corrections); add to it
-  // deterministic coarse-fine update (FP64): per ghost oct of this level 24
-  // face slots (ghost cell x direction) of 5 values, summed later in a fixed
-  // order by coarse_gather_kernel; null: atomic adds into the fathers
+  // deterministic coarse-fine update: per ghost oct of this level 24 face
+  // slots (ghost cell x direction) of 5 values, summed later in a fixed order
+  // by the coarse gather kernels; null: atomic adds into the fathers
   double* gface;
   long long gface_base;    // state entry of the level's first ghost oct
 };
@@ -172,7 +172,14 @@ __device__ __forceinline__ void coarse_add_f64(const LevelArgs& A, double* unew,
   for (int n = 0; n < 5; ++n) atomicAdd(o + 8 * n, sign * (f[n] * 0.125));
 }
 __device__ __forceinline__ void coarse_add_f32(const LevelArgs& A, float* unew_f, double* unew_e, int ghost_ent,
-                                               const float* f, float sign) {
+                                               const float* f, float sign, int slot) {
+  if (A.gface) {  // the face's slot (as coarse_add_f64), the values the atomics would add
+    double* s = A.gface + ((size_t)(ghost_ent - A.gface_base) * 24 + slot) * 5;
+#pragma unroll
+    for (int n = 0; n < 4; ++n) s[n] = (double)(sign * (f[n] * 0.125f));
+    s[4] = (double)sign * ((double)f[4] * 0.125);
+    return;
+  }
   const int2 fa = A.ghost_father[ghost_ent - A.ghost_base];
   if (fa.x < 0) return;
   float* o = unew_f + (size_t)fa.x * kBulkF + fa.y;

@@ -53,8 +53,11 @@ __device__ __forceinline__ void ctoprim_f32x2(const float* sf, const double* sd,
 // Flux reset and coarse corrections of one x or y face of a layer, per plane
 // (.x plane 2K, .y plane 2K+1); bl/br: status bits (a | b<<8) of the cells
 // left/right of the face, el/er their oct entries.
+// cr / cl: the x, y part of the ghost cell's index when the ghost is on the
+// right (above) or left (below) of the face; dir: 0 x faces, 1 y faces.  The
+// lanes are the two planes (z parity h) of the layer.
 __device__ __forceinline__ void amr_face_f32(const LevelArgs& A, const StateArgs<float>& S, float2* f, uint32_t bl,
-                                             uint32_t br, int el, int er) {
+                                             uint32_t br, int el, int er, int cr, int cl, int dir) {
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const uint32_t l = (bl >> (8 * h)) & 0xffu, r = (br >> (8 * h)) & 0xffu;
@@ -65,8 +68,8 @@ __device__ __forceinline__ void amr_face_f32(const LevelArgs& A, const StateArgs
 #pragma unroll
       for (int n = 0; n < 5; ++n) c[n] = 0.f;
     }
-    if ((l & 2u) && (r & 4u)) coarse_add_f32(A, S.unew_f, S.unew_d, er, c, 1.f);
-    if ((l & 4u) && (r & 2u)) coarse_add_f32(A, S.unew_f, S.unew_d, el, c, -1.f);
+    if ((l & 2u) && (r & 4u)) coarse_add_f32(A, S.unew_f, S.unew_d, er, c, 1.f, 3 * (cr + 4 * h) + dir);
+    if ((l & 4u) && (r & 2u)) coarse_add_f32(A, S.unew_f, S.unew_d, el, c, -1.f, 3 * (cl + 4 * h) + dir);
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
       if (h) f[n].y = c[n];

@@ -108,6 +108,12 @@ struct Context {
   std::vector<double> cfl_keys;    // [levelmax+1][8]: parameters of each level's cached CFL values
   // timing of the last godunov launch (for the bench)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // rh_coarse_step prolongs every level's ghost octs ahead, on `side`; a level
+  // whose flag is set waits for its event instead of prolonging in launch_level
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_side_start = nullptr;
+  std::vector<cudaEvent_t> ev_prolong;
+  std::vector<char> prolonged;
 };
 
 Context& ctx();
@@ -115,7 +121,7 @@ Context& ctx();
 // coarse-fine levels (rh_amr.cu)
 int build_amr_tables(int l, const TileCfg& cfg, long long gbase);
 int upload_amr_tables(int l);
-int prolong_ghosts(int l, double smallr);
+int prolong_ghosts(int l, double smallr, cudaStream_t st = nullptr);  // null: the library stream
 // coarse-fine levels built on the device (rh_amr_tables.cu): same tables as
 // build_amr_tables; *d_gfather_out receives the level's ghost fathers (device)
 int build_amr_tables_device(int l, const TileCfg& cfg, long long gbase, const rh_oct* d_grid, int2** d_gfather_out);

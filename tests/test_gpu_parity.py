@@ -387,10 +387,12 @@ def test_amr_sedov_levels3to5_independent_runs_24_steps(prec):
         gpu.close()
 
 
-def test_amr_deterministic_coarse_update_repeats_bitwise():
-    """rh_set_deterministic(1): the FP64 coarse-fine corrections go through
+@pytest.mark.parametrize("prec", ["fp64", "fp32_bulk"])
+def test_amr_deterministic_coarse_update_repeats_bitwise(prec):
+    """rh_set_deterministic(1): the coarse-fine corrections go through
     per-face slots summed in a fixed order, so two AMR runs of four coarse
-    steps are bitwise equal, and each stays within 1e-12 of the oracle."""
+    steps are bitwise equal, and each stays within 1e-12 of the oracle (FP64;
+    FP32-bulk: density 1e-5)."""
     m, P = amr_case("outflow", 1, 0)
     u0 = m.uold.copy()
     o = oracle.OracleHydro(m, P, nthreads=NTHREADS)
@@ -401,14 +403,17 @@ def test_amr_deterministic_coarse_update_repeats_bitwise():
     runs = []
     for _ in range(2):
         m.uold[:] = u0
-        gpu = GodunovGPU(m, P, precision="fp64", deterministic=True)
+        gpu = GodunovGPU(m, P, precision=prec, deterministic=True)
         try:
             states = []
             for s in range(4):
                 gpu.coarse_step()
                 states.append(gpu.fetch_uold())
                 err = rel_l1(states[-1], refs[s])
-                assert np.all(err <= TOL_FP64), (s, err)
+                if prec == "fp64":
+                    assert np.all(err <= TOL_FP64), (s, err)
+                else:
+                    assert err[0] <= TOL_FP32_RHO, (s, err)
         finally:
             gpu.close()
         runs.append(states)
