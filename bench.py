@@ -464,19 +464,19 @@ def bench_amr(args, rank, world, dist, device):
                      "ms_each_step": [round(v, 3) for v in per],
                      "ms_per_coarse_step_python_leaf_calls": float(np.mean(per_calls))}
     out["fp32_bulk_over_fp64"] = out["fp64"]["ms_per_coarse_step"] / out["fp32_bulk"]["ms_per_coarse_step"]
-    # FP64 with the deterministic coarse-fine update (rh_set_deterministic):
-    # its cost, and two runs of 10 coarse steps from the same state compared bit for bit
-    det_ms, finals = [], []
-    for _ in range(2):
-        m.uold[:] = u0
-        gpu = GodunovGPU(m, P, precision="fp64", device=device, deterministic=True)
-        gpu.coarse_step()
-        gpu.push_uold(u0)
-        det_ms.append(float(np.mean([_timed(L, lambda: gpu.coarse_step()) for _ in range(10)])))
-        finals.append(gpu.fetch_uold())
-        gpu.close()
-    out["fp64_deterministic"] = {"ms_per_coarse_step": max_over_ranks([min(det_ms)], dist)[0], "steps": 10,
-                                 "two_runs_bitwise_equal": bool(np.array_equal(finals[0], finals[1]))}
+    # the coarse step's corrections to father cells are summed in a fixed
+    # order: two runs of 10 coarse steps from the same state, compared bit for bit
+    out["repeat_bitwise"] = {}
+    for prec in ("fp64", "fp32_bulk"):
+        finals = []
+        for _ in range(2):
+            m.uold[:] = u0
+            gpu = GodunovGPU(m, P, precision=prec, device=device)
+            for _ in range(10):
+                gpu.coarse_step()
+            finals.append(gpu.fetch_uold())
+            gpu.close()
+        out["repeat_bitwise"][prec] = bool(np.array_equal(finals[0], finals[1]))
     m.uold[:] = u0
     out["_mesh"] = (m, P, u0, fp64_traj if keep_states else None)
     return out

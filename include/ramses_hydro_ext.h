@@ -52,13 +52,20 @@ int rh_level_ghosts(int ilevel, int* gsrc_oct, unsigned char* gsrc_cf, int* gfat
  * set_uold one swap of the two state buffers
  * after all Godunov steps and the restrictions follow, finest first: no
  * Godunov step reads a level that an earlier set_uold or restriction of the
- * step would have changed. */
+ * step would have changed.  On such a mesh the levels' steps run at once on
+ * separate streams (each writes its own cells of unew from uold), every
+ * level's ghost octs are prolonged ahead, and the coarse-fine corrections
+ * are added to the father cells after all steps, in a fixed order: results
+ * repeat bit for bit. */
 int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl);
 
 /* Coarse-fine update of the father cells (unew of level l-1 += or -= the
  * flux/8 of every face between a cell of level l and an interpolated ghost,
- * hydro/godunov_fine.f90:893-1052).  0 (the default): atomic FP64 adds from
- * the pencil kernels, whose order between pencils varies from run to run.
+ * hydro/godunov_fine.f90:893-1052) in the level-by-level calls (rh_godunov)
+ * and in rh_coarse_step on meshes with spare octs; rh_coarse_step on a mesh
+ * whose levels hold every oct always sums them in a fixed order.  0 (the
+ * default): atomic adds from the pencil kernels, whose order between pencils
+ * varies from run to run.
  * 1: each face's contribution goes to its own slot and one thread per father
  * cell adds its 24 slots in a fixed order after the level's kernel (the role
  * of the reference's fixed-order flush of cache octs, godunov_fine.f90:

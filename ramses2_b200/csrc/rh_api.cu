@@ -249,6 +249,8 @@ static void free_tables(LevelTables& t) {
 static void free_state() {
   Context& c = ctx();
   free_host_schedule();
+  cudaFree(c.d_gface_all);
+  c.d_gface_all = nullptr;
   for (auto& t : c.levels) free_tables(t);
   c.levels.clear();
   for (int i = 0; i < 2; ++i) {
@@ -378,6 +380,7 @@ int rh_init(int device_ordinal) {
   RH_CUDA(cudaEventCreate(&c.ev0));
   RH_CUDA(cudaEventCreate(&c.ev1));
   RH_CUDA(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+  for (auto& s : c.lev_stream) RH_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   RH_CUDA(cudaEventCreateWithFlags(&c.ev_side_start, cudaEventDisableTiming));
   c.inited = true;
   return RH_OK;
@@ -396,8 +399,10 @@ int rh_finalize(void) {
   cudaEventDestroy(c.ev0);
   cudaEventDestroy(c.ev1);
   for (cudaEvent_t e : c.ev_prolong) cudaEventDestroy(e);
+  for (cudaEvent_t e : c.ev_level) cudaEventDestroy(e);
   cudaEventDestroy(c.ev_side_start);
   cudaStreamDestroy(c.side);
+  for (auto s : c.lev_stream) cudaStreamDestroy(s);
   cudaStreamDestroy(c.stream);
   c = Context();
   return RH_OK;
@@ -938,7 +943,8 @@ int ensure_level_tables(int l) {
 // partial slots; no partial reduction): rh_coarse_step_host launches a level
 // group by group that way.
 int launch_level(int l, double gamma, double smallr, double smallc, double dt, double dx, double smax_cap,
-                 int slope, int riemann, const double* g, bool fuse_cfl, bool accumulate, const PencilRange* range) {
+                 int slope, int riemann, const double* g, bool fuse_cfl, bool accumulate, const PencilRange* range,
+                 const LevelSlots* slots) {
   Context& c = ctx();
   LevelTables& T = c.levels[l];
   const bool amr = c.nlevels_used > 1;  // refined cells / coarse-fine faces exist on every level
@@ -956,13 +962,14 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
               T.cfg.tyo, want.minb, slope, riemann, amr ? 1 : 0);
     return RH_EINVAL;
   }
+  cudaStream_t st = range && range->stream ? range->stream : (slots && slots->stream ? slots->stream : c.stream);
   if (amr) {
     if (l < (int)c.prolonged.size() && c.prolonged[l]) {
       // prolonged ahead on the side stream by rh_coarse_step
-      RH_CUDA(cudaStreamWaitEvent(c.stream, c.ev_prolong[l], 0));
+      RH_CUDA(cudaStreamWaitEvent(st, c.ev_prolong[l], 0));
       c.prolonged[l] = 0;
     } else {
-      int rc = prolong_ghosts(l, smallr);
+      int rc = prolong_ghosts(l, smallr, st);
       if (rc) return rc;
     }
   }
@@ -989,9 +996,9 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
   A.refmask = c.d_refmask;
   A.ghost_father = c.d_gfather;
   A.accumulate = accumulate ? 1 : 0;
-  A.gface = nullptr;
-  A.gface_base = T.gbase;
-  const bool gather = amr && c.deterministic && T.nghost > 0;
+  A.gface = slots ? slots->gface : nullptr;
+  A.gface_base = slots ? slots->base : T.gbase;
+  const bool gather = !slots && amr && c.deterministic && T.nghost > 0;
   if (gather) {
     const size_t need = (size_t)T.nghost * 24 * 5;
     if (c.gface_elems < need) {
@@ -1020,7 +1027,7 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
     H.zero = 0.0; H.half = 0.5; H.two = 2.0;
     H.gm1 = gamma - 1.0; H.smalle = A.smalle_d;
     for (int d = 0; d < 3; ++d) H.grav[d] = gh[d];
-    RH_CUDA(fn(A, &S, &H, nblocks, range && range->stream ? range->stream : c.stream));
+    RH_CUDA(fn(A, &S, &H, nblocks, st));
   } else {
     StateArgs<float> S{c.ud[c.cur], c.uf[c.cur], c.ud[nxt], c.uf[nxt]};
     HydroK<float2> H;
@@ -1033,7 +1040,7 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
     H.zero = b(0.0); H.half = b(0.5); H.two = b(2.0);
     H.gm1 = b(gamma - 1.0); H.smalle = b(A.smalle_d);
     for (int d = 0; d < 3; ++d) H.grav[d] = b(gh[d]);
-    RH_CUDA(fn(A, &S, &H, nblocks, range && range->stream ? range->stream : c.stream));
+    RH_CUDA(fn(A, &S, &H, nblocks, st));
   }
   if (gather) {
     const unsigned nb = (unsigned)((T.nghost * 5ll + 255) / 256);
@@ -1046,7 +1053,7 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
     RH_CUDA(cudaGetLastError());
   }
   if (fuse_cfl && !range) {
-    reduce_partials_kernel<<<1, 1024, 0, c.stream>>>(T.d_cfl_partial, T.npencil, A.cfl.cdx_smallc, c.d_cfl + 5 * l);
+    reduce_partials_kernel<<<1, 1024, 0, st>>>(T.d_cfl_partial, T.npencil, A.cfl.cdx_smallc, c.d_cfl + 5 * l);
     RH_CUDA(cudaGetLastError());
   }
   return RH_OK;
@@ -1291,50 +1298,74 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
       c.prolonged[l] = 1;
     }
   }
-  // several levels that together hold every oct of the state: set_unew as
-  // one copy of the whole state, set_uold as one buffer swap after all Godunov
-  // steps (below); otherwise level by level
+  // Several levels that together hold every oct of the state: every level's
+  // step reads only uold (its own level and, for its ghosts, the coarser
+  // one) and writes its own cells of unew as uold plus its flux differences,
+  // so the levels run at once on separate streams and no set_unew copy is
+  // needed; the face contributions to father cells (±F/8) go to slots, added
+  // to the fathers' unew afterwards in a fixed order (the deterministic
+  // coarse-fine update, always on here); one swap of the state buffers then
+  // stands for the per-level set_uold copies, and the restrictions follow,
+  // finest first.  Otherwise level by level.
   long long covered = 0;
   for (int l : lev) covered += c.noct[l];
   const bool swap_all = lev.size() > 1 && covered == c.ngridmax;
   if (swap_all) {
-    if ((rc = copy_level(1, c.ngridmax, c.cur, 1 - c.cur))) return rc;
-    for (int l : lev) {
-      c.unew_copied[l] = 1;
-      c.unew_pending[l] = 0;
-      c.unew_written[l] = 0;
+    const long long nghost_all = c.nstate - c.ngridmax;
+    if (nghost_all > 0 && !c.d_gface_all) {
+      // zeroed once: the slots a step writes are fixed by the mesh, each
+      // written in full every step, and the others stay zero
+      RH_CUDA(cudaMalloc(&c.d_gface_all, sizeof(double) * 120 * nghost_all));
+      RH_CUDA(cudaMemsetAsync(c.d_gface_all, 0, sizeof(double) * 120 * nghost_all, c.stream));
     }
-  } else {
-    for (int l : lev)
-      if ((rc = rh_set_unew(c.head[l], c.noct[l]))) return rc;
-  }
-  for (size_t i = lev.size(); i-- > 0;) {
-    const int l = lev[i];
-    const double dx = dxl(l);
-    rc = rh_godunov((c.head[l] - 1) / n3 + 1, c.noct[l] / n3, c.ngridmax, l, c.levelmin, c.levelmax, p->gamma,
-                    p->smallr, p->smallc * p->smallc, step_dt, dx, p->courant_factor * dx / step_dt, p->slope_type,
-                    p->riemann, c.gravity);
-    if (rc) return rc;
-    if (!swap_all && (rc = rh_set_uold(c.head[l], c.noct[l]))) return rc;
-    if (!swap_all && i + 1 < lev.size() && l + 1 <= c.levelmax && c.noct[l + 1] > 0) {
-      rc = rh_upload(c.head[l + 1], c.noct[l + 1], p->interpol_var == 1 ? 1 : 0, p->gamma, p->smallr,
-                     p->smallc * p->smallc);
+    if (c.ev_level.size() < (size_t)(c.levelmax + 1)) {
+      for (size_t k = c.ev_level.size(); k < (size_t)(c.levelmax + 1); ++k) {
+        cudaEvent_t e;
+        RH_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c.ev_level.push_back(e);
+      }
+    }
+    RH_CUDA(cudaEventRecord(c.ev_side_start, c.stream));
+    for (auto s : c.lev_stream) RH_CUDA(cudaStreamWaitEvent(s, c.ev_side_start, 0));
+    std::vector<char> fused(c.levelmax + 1, 0), corrected(c.levelmax + 1, 0);
+    int j = 0;
+    for (size_t i = lev.size(); i-- > 0; ++j) {
+      const int l = lev[i];
+      const double dx = dxl(l);
+      if (l > c.levelmin && c.levels[l].nghost > 0) corrected[l - 1] = 1;
+      const double* key = &c.cfl_keys[8 * l];
+      fused[l] = key[0] == dx && key[1] == p->gamma && key[2] == p->smallr && key[5] == c.gravity[0] &&
+                 key[6] == c.gravity[1] && key[7] == c.gravity[2] && key[3] == p->smallc;
+      cudaStream_t st = j == 0 ? c.stream : c.lev_stream[(j - 1) % 3];
+      const LevelSlots S{c.d_gface_all, c.ngridmax, st};
+      rc = launch_level(l, p->gamma, p->smallr, p->smallc, step_dt, dx, p->courant_factor * dx / step_dt,
+                        p->slope_type, p->riemann, c.gravity, fused[l] != 0, false, nullptr, &S);
       if (rc) return rc;
+      RH_CUDA(cudaEventRecord(c.ev_level[l], st));
     }
-  }
-  if (swap_all) {
-    // Every level's unew is complete (set_unew's copy, the coarse corrections
-    // of the finer level, the level's own update), and no Godunov step of the
-    // loop above read a level whose set_uold or restriction the reference
-    // makes before it (each reads its own level and, for ghosts, the coarser
-    // one, both still old): one swap of the state buffers stands for the
-    // per-level set_uold copies, then the restrictions, finest first.
+    for (int l : lev) RH_CUDA(cudaStreamWaitEvent(c.stream, c.ev_level[l], 0));
+    // the coarse-fine corrections, level by level into the coarser level's unew
+    for (int l : lev) {
+      const LevelTables& T = c.levels[l];
+      if (T.nghost == 0) continue;
+      const unsigned nb = (unsigned)((T.nghost * 5ll + 255) / 256);
+      const double* slots = c.d_gface_all + (size_t)(T.gbase - c.ngridmax) * 120;
+      if (c.precision == RH_PREC_FP64)
+        coarse_gather_kernel<<<nb, 256, 0, c.stream>>>(slots, T.nghost, c.d_gfather + (T.gbase - c.ngridmax),
+                                                       c.ud[1 - c.cur]);
+      else
+        coarse_gather_f32_kernel<<<nb, 256, 0, c.stream>>>(slots, T.nghost, c.d_gfather + (T.gbase - c.ngridmax),
+                                                           c.uf[1 - c.cur], c.ud[1 - c.cur]);
+      RH_CUDA(cudaGetLastError());
+    }
     c.cur = 1 - c.cur;
     for (int l : lev) {
       c.unew_pending[l] = 0;
       c.unew_written[l] = 0;
       c.unew_copied[l] = 0;
-      c.cfl_on_uold[l] = c.cfl_on_unew[l];
+      // a level whose father cells received corrections after its fused CFL
+      // epilogue ran gets its courant_fine values recomputed next time
+      c.cfl_on_uold[l] = fused[l] && !corrected[l];
       c.cfl_on_unew[l] = 0;
     }
     for (size_t i = lev.size() - 1; i-- > 0;) {
@@ -1344,6 +1375,25 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
                        p->smallc * p->smallc);
         if (rc) return rc;
       }
+    }
+    *dt = step_dt;
+    if (c.state_check) return check_all_levels();
+    return RH_OK;
+  }
+  for (int l : lev)
+    if ((rc = rh_set_unew(c.head[l], c.noct[l]))) return rc;
+  for (size_t i = lev.size(); i-- > 0;) {
+    const int l = lev[i];
+    const double dx = dxl(l);
+    rc = rh_godunov((c.head[l] - 1) / n3 + 1, c.noct[l] / n3, c.ngridmax, l, c.levelmin, c.levelmax, p->gamma,
+                    p->smallr, p->smallc * p->smallc, step_dt, dx, p->courant_factor * dx / step_dt, p->slope_type,
+                    p->riemann, c.gravity);
+    if (rc) return rc;
+    if ((rc = rh_set_uold(c.head[l], c.noct[l]))) return rc;
+    if (i + 1 < lev.size() && l + 1 <= c.levelmax && c.noct[l + 1] > 0) {
+      rc = rh_upload(c.head[l + 1], c.noct[l + 1], p->interpol_var == 1 ? 1 : 0, p->gamma, p->smallr,
+                     p->smallc * p->smallc);
+      if (rc) return rc;
     }
   }
   *dt = step_dt;

@@ -114,6 +114,10 @@ struct Context {
   cudaEvent_t ev_side_start = nullptr;
   std::vector<cudaEvent_t> ev_prolong;
   std::vector<char> prolonged;
+  // rh_coarse_step's levels run concurrently on the library stream and these
+  cudaStream_t lev_stream[3] = {nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> ev_level;
+  double* d_gface_all = nullptr;  // [ghost octs of the mesh][24][5], zeroed once per mesh
 };
 
 Context& ctx();
@@ -143,11 +147,19 @@ struct PencilRange {
   int n;
   cudaStream_t stream;  // stream of the launch (the library stream when null)
 };
+// A level step of rh_coarse_step's concurrent path: coarse-fine face
+// contributions go to the all-level slot buffer (entry e's slots at
+// (e - base) * 24), no per-level gather, launched on `stream`.
+struct LevelSlots {
+  double* gface;
+  long long base;
+  cudaStream_t stream;
+};
 // rh_api.cu: one Godunov step of level l (all pencils, or `range`'s), and the
 // FP64 staging buffer of FP32-bulk transfers (grown on demand, kept).
 int launch_level(int l, double gamma, double smallr, double smallc, double dt, double dx, double smax_cap,
                  int slope, int riemann, const double* g, bool fuse_cfl, bool accumulate = false,
-                 const PencilRange* range = nullptr);
+                 const PencilRange* range = nullptr, const LevelSlots* slots = nullptr);
 int stage64(long long noct, double** out);
 int ensure_level_tables(int l);
 TileCfg level_cfg(int l);  // tile of level l's launches (see rh_api.cu)
