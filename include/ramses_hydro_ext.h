@@ -48,15 +48,17 @@ int rh_level_ghosts(int ilevel, int* gsrc_oct, unsigned char* gsrc_cf, int* gfat
  * the courant_fine values of each level.  The same results as the separate
  * calls, without a host round trip per call (the reference's host makes them
  * one by one; this is for hosts that step whole meshes).  When the levels
- * hold every oct of the state, set_unew is one copy of the whole state and
- * set_uold one swap of the two state buffers
- * after all Godunov steps and the restrictions follow, finest first: no
- * Godunov step reads a level that an earlier set_uold or restriction of the
- * step would have changed.  On such a mesh the levels' steps run at once on
- * separate streams (each writes its own cells of unew from uold), every
- * level's ghost octs are prolonged ahead, and the coarse-fine corrections
- * are added to the father cells after all steps, in a fixed order: results
- * repeat bit for bit. */
+ * hold every oct of the state, the levels' steps run at once on separate
+ * streams (each writes its own cells of unew from uold, so no set_unew copy
+ * is needed), every level's ghost octs are prolonged ahead, the coarse-fine
+ * corrections are added to the father cells after all steps in a fixed order
+ * (results repeat bit for bit), set_uold is one swap of the two state
+ * buffers and the restrictions follow, finest first: no Godunov step reads a
+ * level that an earlier set_uold or restriction of the step would have
+ * changed.  There the step also leaves every level's courant_fine values of
+ * the new state (the pencils' fused epilogue for the cells they finish, the
+ * correcting gather for the father cells), so the next call's rh_cmpdt of
+ * every level reads five numbers instead of the state. */
 int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl);
 
 /* Coarse-fine update of the father cells (unew of level l-1 += or -= the

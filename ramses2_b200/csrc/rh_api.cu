@@ -142,15 +142,9 @@ __global__ void cmpdt_kernel(const double* __restrict__ ud, const float* __restr
     long long oct = oct0 + cell_id / 8;
     int cell = (int)(cell_id % 8);
     const bool ref = refined ? refined[cell_id] != 0 : (refbits ? ((refbits[oct] >> cell) & 1) != 0 : false);
-    if (!ref) {
-      double r, m1, m2, m3, E;
-      if (!fp32) {
-        const double* o = ud + oct * 40 + cell;
-        r = o[0]; m1 = o[8]; m2 = o[16]; m3 = o[24]; E = o[32];
-      } else {
-        const float* o = uf + oct * kBulkF + cell;
-        r = o[0]; m1 = o[8]; m2 = o[16]; m3 = o[24]; E = ud[oct * kBulkD + cell];
-      }
+    if (!ref && !fp32) {
+      const double* o = ud + oct * 40 + cell;
+      const double r = o[0], m1 = o[8], m2 = o[16], m3 = o[24], E = o[32];
       m = r * vol;
       ek = E * vol;
       const double rm = r > C.smallr ? r : C.smallr;
@@ -159,6 +153,17 @@ __global__ void cmpdt_kernel(const double* __restrict__ ud, const float* __restr
       ei -= 0.5 * (m2 * m2) / rm * vol;
       ei -= 0.5 * (m3 * m3) / rm * vol;
       dt = cmpdt_cell(r, m1, m2, m3, E, C);
+    } else if (!ref) {
+      // an FP32-bulk cell in the fused epilogue's FP32-bulk form, so that a
+      // level's values do not depend on which of the two computed them
+      const float* o = uf + oct * kBulkF + cell;
+      CflAcc a;
+      a.add_bulk(o[0], o[8], o[16], o[24], ud[oct * kBulkD + cell], C);
+      a.scale_bulk(vol);
+      m = a.mass;
+      ek = a.ekin;
+      ei = a.eint;
+      dt = a.dt(C);
     }
   }
   for (int off = 16; off > 0; off >>= 1) {
@@ -251,6 +256,10 @@ static void free_state() {
   free_host_schedule();
   cudaFree(c.d_gface_all);
   c.d_gface_all = nullptr;
+  cudaFree(c.d_cflskip);
+  c.d_cflskip = nullptr;
+  cudaFree(c.d_gcfl);
+  c.d_gcfl = nullptr;
   for (auto& t : c.levels) free_tables(t);
   c.levels.clear();
   for (int i = 0; i < 2; ++i) {
@@ -924,6 +933,139 @@ __global__ void coarse_gather_f32_kernel(const double* __restrict__ gface, int n
   }
 }
 
+// The concurrent coarse step's coarse-fine update with the courant_fine
+// values of the cells it corrects.  The fused CFL epilogue of a level leaves
+// out its cells that father a finer level's ghost octs (LevelArgs::cflskip):
+// their state is final only once the finer level's face slots are added.
+// Here one thread per (ghost, variable) adds them in slot order exactly as
+// coarse_gather_kernel does, 64 ghosts per block, and one thread per ghost
+// then takes its father cell's new state into the block's CFL partial (the
+// cell as courant_fine sees it: the stored values, FP32 ones in FP32-bulk).
+// The level's pencil partials and these together cover each of its leaf
+// cells once.
+constexpr int kGatherGhosts = 64;
+constexpr int kGatherThreads = kGatherGhosts * 5;
+
+__global__ void __launch_bounds__(kGatherThreads)
+    coarse_gather_cfl_kernel(const double* __restrict__ gface, int nghost, const int2* __restrict__ fathers,
+                             const uint8_t* __restrict__ refmask, double* __restrict__ unew, CflConst C, double vol,
+                             double* __restrict__ partial) {
+  __shared__ double cell[kGatherGhosts][5];
+  __shared__ double red[kGatherThreads / 32 * 4];
+  const int lg = threadIdx.x / 5, v = threadIdx.x - 5 * lg;
+  const long long g = (long long)blockIdx.x * kGatherGhosts + lg;
+  if (g < nghost) {
+    const int2 fa = fathers[g];
+    if (fa.x >= 0) {
+      const double* s = gface + (size_t)g * 24 * 5 + v;
+      double sum = 0.0;
+#pragma unroll 4
+      for (int f = 0; f < 24; ++f) sum += s[5 * f];
+      double* o = unew + (size_t)fa.x * 40 + 8 * v + fa.y;
+      const double nv = *o + sum;
+      *o = nv;
+      cell[lg][v] = nv;
+    }
+  }
+  __syncthreads();
+  CflAcc acc;
+  if (threadIdx.x < kGatherGhosts) {
+    const long long gg = (long long)blockIdx.x * kGatherGhosts + threadIdx.x;
+    if (gg < nghost) {
+      const int2 fa = fathers[gg];
+      if (fa.x >= 0 && !((refmask[fa.x] >> fa.y) & 1u)) {
+        const double* q = cell[threadIdx.x];
+        acc.add(q[0], q[1], q[2], q[3], q[4], C, vol);
+      }
+    }
+  }
+  cfl_block_reduce<kGatherThreads / 32>(acc, C, red, partial + (size_t)blockIdx.x * 5);
+}
+
+__global__ void __launch_bounds__(kGatherThreads)
+    coarse_gather_cfl_f32_kernel(const double* __restrict__ gface, int nghost, const int2* __restrict__ fathers,
+                                 const uint8_t* __restrict__ refmask, float* __restrict__ unew_f,
+                                 double* __restrict__ unew_e, CflConst C, double vol, double* __restrict__ partial) {
+  __shared__ double cell[kGatherGhosts][5];
+  __shared__ double red[kGatherThreads / 32 * 4];
+  const int lg = threadIdx.x / 5, v = threadIdx.x - 5 * lg;
+  const long long g = (long long)blockIdx.x * kGatherGhosts + lg;
+  if (g < nghost) {
+    const int2 fa = fathers[g];
+    if (fa.x >= 0) {
+      const double* s = gface + (size_t)g * 24 * 5 + v;
+      double sum = 0.0;
+#pragma unroll 4
+      for (int f = 0; f < 24; ++f) sum += s[5 * f];
+      if (v < 4) {
+        float* o = unew_f + (size_t)fa.x * kBulkF + 8 * v + fa.y;
+        const float nv = (float)((double)*o + sum);
+        *o = nv;
+        cell[lg][v] = nv;
+      } else {
+        double* o = unew_e + (size_t)fa.x * kBulkD + fa.y;
+        const double nv = *o + sum;
+        *o = nv;
+        cell[lg][4] = nv;
+      }
+    }
+  }
+  __syncthreads();
+  CflAcc acc;
+  if (threadIdx.x < kGatherGhosts) {
+    const long long gg = (long long)blockIdx.x * kGatherGhosts + threadIdx.x;
+    if (gg < nghost) {
+      const int2 fa = fathers[gg];
+      if (fa.x >= 0 && !((refmask[fa.x] >> fa.y) & 1u)) {
+        const double* q = cell[threadIdx.x];
+        acc.add_bulk((float)q[0], (float)q[1], (float)q[2], (float)q[3], q[4], C);
+      }
+    }
+  }
+  acc.scale_bulk(vol);
+  cfl_block_reduce<kGatherThreads / 32>(acc, C, red, partial + (size_t)blockIdx.x * 5);
+}
+
+// Bit fa.y of byte fa.x for every ghost's father cell (the byte array read
+// as 32-bit words, zeroed before).
+__global__ void mark_fathers_kernel(const int2* __restrict__ fathers, int nghost, unsigned* __restrict__ mask) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (g >= nghost) return;
+  const int2 fa = fathers[g];
+  if (fa.x < 0) return;
+  atomicOr(mask + (fa.x >> 2), 1u << (8 * (fa.x & 3) + fa.y));
+}
+
+// reduce_partials_kernel over two partial arrays taken as one (a level's
+// pencil partials followed by its corrected cells' gather partials).
+__global__ void reduce_partials_pair_kernel(const double* __restrict__ p1, long long n1,
+                                            const double* __restrict__ p2, long long n2, double dt0,
+                                            double* __restrict__ out) {
+  __shared__ double red[1024][4];
+  double a = 0, b = 0, c = 0, d = 1e300;
+  for (long long i = threadIdx.x; i < n1 + n2; i += blockDim.x) {
+    const double* q = i < n1 ? p1 + i * 5 : p2 + (i - n1) * 5;
+    a += q[0]; b += q[1]; c += q[2];
+    d = q[4] < d ? q[4] : d;
+  }
+  red[threadIdx.x][0] = a; red[threadIdx.x][1] = b; red[threadIdx.x][2] = c; red[threadIdx.x][3] = d;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      red[threadIdx.x][0] += red[threadIdx.x + s][0];
+      red[threadIdx.x][1] += red[threadIdx.x + s][1];
+      red[threadIdx.x][2] += red[threadIdx.x + s][2];
+      double o = red[threadIdx.x + s][3];
+      red[threadIdx.x][3] = o < red[threadIdx.x][3] ? o : red[threadIdx.x][3];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = red[0][0]; out[1] = red[0][1]; out[2] = red[0][2]; out[3] = 0.0;
+    out[4] = red[0][3] < dt0 ? red[0][3] : dt0;
+  }
+}
+
 // Pencil tables of level l for the tile the level's launches use (built, or
 // rebuilt after a tile change, on demand).
 int ensure_level_tables(int l) {
@@ -998,6 +1140,7 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
   A.accumulate = accumulate ? 1 : 0;
   A.gface = slots ? slots->gface : nullptr;
   A.gface_base = slots ? slots->base : T.gbase;
+  A.cflskip = slots ? slots->cflskip : nullptr;
   const bool gather = !slots && amr && c.deterministic && T.nghost > 0;
   if (gather) {
     const size_t need = (size_t)T.nghost * 24 * 5;
@@ -1052,7 +1195,7 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
                                                          c.uf[nxt], c.ud[nxt]);
     RH_CUDA(cudaGetLastError());
   }
-  if (fuse_cfl && !range) {
+  if (fuse_cfl && !range && !(slots && slots->defer_reduce)) {
     reduce_partials_kernel<<<1, 1024, 0, st>>>(T.d_cfl_partial, T.npencil, A.cfl.cdx_smallc, c.d_cfl + 5 * l);
     RH_CUDA(cudaGetLastError());
   }
@@ -1317,6 +1460,20 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
       // written in full every step, and the others stay zero
       RH_CUDA(cudaMalloc(&c.d_gface_all, sizeof(double) * 120 * nghost_all));
       RH_CUDA(cudaMemsetAsync(c.d_gface_all, 0, sizeof(double) * 120 * nghost_all, c.stream));
+      // the father cells of every level's ghosts, and room for the gathers' CFL partials
+      const size_t mask_bytes = ((size_t)c.ngridmax + 3) / 4 * 4;
+      RH_CUDA(cudaMalloc(&c.d_cflskip, mask_bytes));
+      RH_CUDA(cudaMemsetAsync(c.d_cflskip, 0, mask_bytes, c.stream));
+      long long nblk = 0;
+      for (int l : lev) {
+        const LevelTables& T = c.levels[l];
+        if (T.nghost == 0) continue;
+        mark_fathers_kernel<<<(unsigned)((T.nghost + 255) / 256), 256, 0, c.stream>>>(
+            c.d_gfather + (T.gbase - c.ngridmax), T.nghost, reinterpret_cast<unsigned*>(c.d_cflskip));
+        RH_CUDA(cudaGetLastError());
+        nblk += (T.nghost + kGatherGhosts - 1) / kGatherGhosts;
+      }
+      RH_CUDA(cudaMalloc(&c.d_gcfl, sizeof(double) * 5 * (size_t)std::max(1LL, nblk)));
     }
     if (c.ev_level.size() < (size_t)(c.levelmax + 1)) {
       for (size_t k = c.ev_level.size(); k < (size_t)(c.levelmax + 1); ++k) {
@@ -1337,7 +1494,10 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
       fused[l] = key[0] == dx && key[1] == p->gamma && key[2] == p->smallr && key[5] == c.gravity[0] &&
                  key[6] == c.gravity[1] && key[7] == c.gravity[2] && key[3] == p->smallc;
       cudaStream_t st = j == 0 ? c.stream : c.lev_stream[(j - 1) % 3];
-      const LevelSlots S{c.d_gface_all, c.ngridmax, st};
+      // a level whose father cells the gathers correct leaves them to the
+      // gathers' CFL and has its partials reduced together with theirs
+      const bool merge = fused[l] && corrected[l] && c.d_cflskip;
+      const LevelSlots S{c.d_gface_all, c.ngridmax, st, merge ? c.d_cflskip : nullptr, merge};
       rc = launch_level(l, p->gamma, p->smallr, p->smallc, step_dt, dx, p->courant_factor * dx / step_dt,
                         p->slope_type, p->riemann, c.gravity, fused[l] != 0, false, nullptr, &S);
       if (rc) return rc;
@@ -1345,27 +1505,53 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
     }
     for (int l : lev) RH_CUDA(cudaStreamWaitEvent(c.stream, c.ev_level[l], 0));
     // the coarse-fine corrections, level by level into the coarser level's unew
+    long long goff = 0;
     for (int l : lev) {
       const LevelTables& T = c.levels[l];
       if (T.nghost == 0) continue;
-      const unsigned nb = (unsigned)((T.nghost * 5ll + 255) / 256);
       const double* slots = c.d_gface_all + (size_t)(T.gbase - c.ngridmax) * 120;
-      if (c.precision == RH_PREC_FP64)
-        coarse_gather_kernel<<<nb, 256, 0, c.stream>>>(slots, T.nghost, c.d_gfather + (T.gbase - c.ngridmax),
-                                                       c.ud[1 - c.cur]);
-      else
-        coarse_gather_f32_kernel<<<nb, 256, 0, c.stream>>>(slots, T.nghost, c.d_gfather + (T.gbase - c.ngridmax),
-                                                           c.uf[1 - c.cur], c.ud[1 - c.cur]);
-      RH_CUDA(cudaGetLastError());
+      const int2* fathers = c.d_gfather + (T.gbase - c.ngridmax);
+      const int lf = l - 1;  // the fathers' level
+      if (lf >= c.levelmin && fused[lf] && corrected[lf] && c.d_cflskip) {
+        // the father level's CFL constants, as launch_level formed them
+        const double dxf = dxl(lf);
+        const double* lkey = &c.cfl_keys[8 * lf];
+        const double smax_cap = p->courant_factor * dxf / step_dt;
+        const double courant = lkey[4] > 0 ? lkey[4] : smax_cap * step_dt / dxf;
+        const CflConst C = make_cfl(dxf, p->gamma, p->smallr, p->smallc, courant, c.gravity);
+        const double vol = dxf * dxf * dxf;
+        const long long nb = (T.nghost + kGatherGhosts - 1) / kGatherGhosts;
+        double* part = c.d_gcfl + 5 * goff;
+        if (c.precision == RH_PREC_FP64)
+          coarse_gather_cfl_kernel<<<(unsigned)nb, kGatherThreads, 0, c.stream>>>(
+              slots, T.nghost, fathers, c.d_refmask, c.ud[1 - c.cur], C, vol, part);
+        else
+          coarse_gather_cfl_f32_kernel<<<(unsigned)nb, kGatherThreads, 0, c.stream>>>(
+              slots, T.nghost, fathers, c.d_refmask, c.uf[1 - c.cur], c.ud[1 - c.cur], C, vol, part);
+        RH_CUDA(cudaGetLastError());
+        const LevelTables& F = c.levels[lf];
+        reduce_partials_pair_kernel<<<1, 1024, 0, c.stream>>>(F.d_cfl_partial, F.npencil, part, nb,
+                                                              C.cdx_smallc, c.d_cfl + 5 * lf);
+        RH_CUDA(cudaGetLastError());
+        goff += nb;
+      } else {
+        const unsigned nb = (unsigned)((T.nghost * 5ll + 255) / 256);
+        if (c.precision == RH_PREC_FP64)
+          coarse_gather_kernel<<<nb, 256, 0, c.stream>>>(slots, T.nghost, fathers, c.ud[1 - c.cur]);
+        else
+          coarse_gather_f32_kernel<<<nb, 256, 0, c.stream>>>(slots, T.nghost, fathers, c.uf[1 - c.cur],
+                                                             c.ud[1 - c.cur]);
+        RH_CUDA(cudaGetLastError());
+      }
     }
     c.cur = 1 - c.cur;
     for (int l : lev) {
       c.unew_pending[l] = 0;
       c.unew_written[l] = 0;
       c.unew_copied[l] = 0;
-      // a level whose father cells received corrections after its fused CFL
-      // epilogue ran gets its courant_fine values recomputed next time
-      c.cfl_on_uold[l] = fused[l] && !corrected[l];
+      // every fused level's courant_fine values are complete: a corrected
+      // level's own partials plus its corrected cells' from the gathers
+      c.cfl_on_uold[l] = fused[l];
       c.cfl_on_unew[l] = 0;
     }
     for (size_t i = lev.size() - 1; i-- > 0;) {

@@ -150,15 +150,14 @@ __global__ void batch_cfl_kernel(BatchProb P, const double* ud, const float* uf,
   if (i < noct * 8) {
     const long long o = P.oct0 + (i >> 3);
     const int cell = (int)(i & 7);
-    double r, m1, m2, m3, E;
     if (!fp32) {
       const double* p = ud + o * 40 + cell;
-      r = p[0]; m1 = p[8]; m2 = p[16]; m3 = p[24]; E = p[32];
-    } else {
+      acc.add(p[0], p[8], p[16], p[24], p[32], A);
+    } else {  // the FP32-bulk form the fused epilogue of the problem's steps uses
       const float* p = uf + o * kBulkF + cell;
-      r = p[0]; m1 = p[8]; m2 = p[16]; m3 = p[24]; E = ud[o * kBulkD + cell];
+      acc.add_bulk(p[0], p[8], p[16], p[24], ud[o * kBulkD + cell], A);
+      acc.scale_bulk(A.vol);
     }
-    acc.add(r, m1, m2, m3, E, A);
   }
   double v[4] = {acc.mass, acc.ekin, acc.eint, acc.dt(A.cfl)};
   for (int off = 16; off > 0; off >>= 1) {

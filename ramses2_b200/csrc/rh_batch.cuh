@@ -92,6 +92,9 @@ __device__ __forceinline__ void batch_level(const BatchProb& P, double dt, int* 
   A.refmask = nullptr;
   A.ghost_father = nullptr;
   A.accumulate = 0;
+  A.gface = nullptr;
+  A.gface_base = 0;
+  A.cflskip = nullptr;
   (void)dt;
 }
 

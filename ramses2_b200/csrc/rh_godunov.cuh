@@ -135,18 +135,29 @@ struct LevelArgs {
   // by the coarse gather kernels; null: atomic adds into the fathers
   double* gface;
   long long gface_base;    // state entry of the level's first ghost oct
+  // per real oct: bit c = cell c is the father of a finer level's ghost oct,
+  // whose courant_fine values the coarse gather computes after its
+  // correction (the fused epilogue leaves those cells out); null: none
+  const uint8_t* cflskip;
 };
 
 // Coarse-fine status of one cell of an AMR level (hydro/godunov_fine.f90:
 // 666-685 flux reset, 893-1052 coarse update): bit 0 refined, bit 1 a cell of
 // this level updated by this pencil, bit 2 an interpolated ghost inside the
-// domain (its father cell receives the face flux / 8).
+// domain (its father cell receives the face flux / 8), bit 3 a cell left out
+// of the fused CFL epilogue (A.cflskip).  The epilogue counts a cell when
+// bits 0 and 3 are clear (mask kNoCfl).
+constexpr uint32_t kNoCfl = 9u;
 __device__ __forceinline__ uint32_t amr_bits(const LevelArgs& A, int ent, int cell, bool upd_pos, bool in_dom) {
   uint32_t b = 0;
   if (ent >= 0) {
     b = (A.refmask[ent] >> cell) & 1u;
-    if (ent < A.ghost_base) b |= upd_pos ? 2u : 0u;
-    else b |= in_dom ? 4u : 0u;
+    if (ent < A.ghost_base) {
+      b |= upd_pos ? 2u : 0u;
+      if (A.cflskip) b |= ((A.cflskip[ent] >> cell) & 1u) << 3;
+    } else {
+      b |= in_dom ? 4u : 0u;
+    }
   }
   return b;
 }
@@ -208,16 +219,19 @@ constexpr long long kWaitBound = 1ll << 22;  // bounded mbarrier spin (seconds a
 struct CflAcc {
   double mass = 0, ekin = 0, eint = 0, cmax = 0;
   __device__ __forceinline__ void add(double r, double m1, double m2, double m3, double E, const LevelArgs& A) {
-    mass += r * A.vol;
-    ekin += E * A.vol;
-    const double rm = r > A.cfl.smallr ? r : A.cfl.smallr;
+    add(r, m1, m2, m3, E, A.cfl, A.vol);
+  }
+  __device__ __forceinline__ void add(double r, double m1, double m2, double m3, double E, const CflConst& C,
+                                      double vol) {
+    mass += r * vol;
+    ekin += E * vol;
+    const double rm = r > C.smallr ? r : C.smallr;
     const double irm = vrcp(rm);
-    double ei = E * A.vol;
-    ei -= 0.5 * (m1 * m1) * irm * A.vol;
-    ei -= 0.5 * (m2 * m2) * irm * A.vol;
-    ei -= 0.5 * (m3 * m3) * irm * A.vol;
+    double ei = E * vol;
+    ei -= 0.5 * (m1 * m1) * irm * vol;
+    ei -= 0.5 * (m2 * m2) * irm * vol;
+    ei -= 0.5 * (m3 * m3) * irm * vol;
     eint += ei;
-    const CflConst& C = A.cfl;
     const double u = m1 * irm, v = m2 * irm, w = m3 * irm;
     double e = E - 0.5 * rm * (u * u);
     e = e - 0.5 * rm * (v * v);
@@ -238,7 +252,10 @@ struct CflAcc {
   // are exact in FP64) and ctot = (|m1| + |m2| + |m3|) / rho + ndim c.
   __device__ __forceinline__ void add_bulk(float rf, float m1f, float m2f, float m3f, double E,
                                            const LevelArgs& A) {
-    const CflConst& C = A.cfl;
+    add_bulk(rf, m1f, m2f, m3f, E, A.cfl);
+  }
+  __device__ __forceinline__ void add_bulk(float rf, float m1f, float m2f, float m3f, double E,
+                                           const CflConst& C) {
     const double r = rf, m1 = m1f, m2 = m2f, m3 = m3f;
     mass += r;
     ekin += E;

@@ -118,6 +118,8 @@ struct Context {
   cudaStream_t lev_stream[3] = {nullptr, nullptr, nullptr};
   std::vector<cudaEvent_t> ev_level;
   double* d_gface_all = nullptr;  // [ghost octs of the mesh][24][5], zeroed once per mesh
+  uint8_t* d_cflskip = nullptr;   // [ngridmax, rounded up to 4] father cells of ghost octs (bit per cell)
+  double* d_gcfl = nullptr;       // [gather blocks of all levels][5] CFL partials of the corrected cells
 };
 
 Context& ctx();
@@ -154,6 +156,8 @@ struct LevelSlots {
   double* gface;
   long long base;
   cudaStream_t stream;
+  const uint8_t* cflskip;  // cells the fused CFL epilogue leaves out (null: none)
+  bool defer_reduce;       // no partial reduction: the caller merges it with the gather's
 };
 // rh_api.cu: one Godunov step of level l (all pencils, or `range`'s), and the
 // FP64 staging buffer of FP32-bulk transfers (grown on demand, kept).

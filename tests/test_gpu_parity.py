@@ -236,7 +236,9 @@ def test_fp32_bulk_courant_fine_on_its_state():
     kernel (FP64 sums and dt over the new FP32 density and momenta and FP64
     energy) and the standalone reduction of the same state re-uploaded both
     match exact sums of the cell terms and the oracle's courant_fine on that
-    state (the fetched values are exact: FP32 widened, FP64 energy)."""
+    state (the fetched values are exact: FP32 widened, FP64 energy).  Both
+    take the cells in the same FP32-bulk form, so their dt is the same
+    number."""
     import math
 
     m = uniform_mesh(5, nsubgrid=1, bc="outflow")
@@ -258,6 +260,7 @@ def test_fp32_bulk_courant_fine_on_its_state():
     lu = u[m.level_slice(5)]
     mass = math.fsum((lu[:, 0, :] * vol).ravel())
     etot = math.fsum((lu[:, 4, :] * vol).ravel())
+    assert fused[4] == alone[4]
     for c in (fused, alone):
         assert c[0] == pytest.approx(mass, rel=1e-13)
         assert c[1] == pytest.approx(etot, rel=1e-13)
@@ -419,6 +422,40 @@ def test_amr_deterministic_coarse_update_repeats_bitwise(prec):
         runs.append(states)
     for a, b in zip(*runs):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32_bulk"])
+def test_amr_coarse_step_courant_values_match_a_fresh_courant_fine(prec):
+    """After each concurrent coarse step every level's courant_fine values
+    come from the step itself: the pencils' fused epilogue for the cells
+    whose state they finish, and the coarse gather for the father cells it
+    corrects afterwards.  They must equal a fresh courant_fine pass over the
+    new state (parameters changed and restored so that nothing is reused):
+    dt bitwise, the mass and energy sums to 1e-13."""
+    from ramses2_b200.mesh import sedov_amr_mesh
+
+    m, g = sedov_amr_mesh(3, 5, radius=0.3)
+    levels = [l for l in range(m.levelmin, m.levelmax + 1) if m.noct[l]]
+    assert len(levels) == 3
+    P = HydroParams.make(gamma=g, courant_factor=0.8, slope_type=2, riemann="hllc", interpol_var=0,
+                         interpol_type=1)
+    gpu = GodunovGPU(m, P, precision=prec)
+    try:
+        for s in range(3):
+            gpu.coarse_step()
+            from_step = {l: gpu.courant_fine(l) for l in levels}
+            fresh = {}
+            for l in levels:
+                gpu.params.courant_factor = 0.5
+                gpu.courant_fine(l)
+                gpu.params.courant_factor = 0.8
+                fresh[l] = gpu.courant_fine(l)
+            for l in levels:
+                a, b = from_step[l], fresh[l]
+                assert a[4] == b[4], (s, l, a, b)
+                np.testing.assert_allclose(a[:3], b[:3], rtol=1e-13, err_msg="step %d level %d" % (s, l))
+    finally:
+        gpu.close()
 
 
 def test_amr_coarse_step_native_given_dt_fp32_bulk():
