@@ -902,9 +902,10 @@ __global__ void coarse_gather_kernel(const double* __restrict__ gface, int nghos
 // coarse-fine tile (kernels that handle refined cells and interpolated ghosts)
 // on every level of a multi-level mesh.  (A level that fills its box could
 // take deeper pencils, with fewer halo layers per cell; on the AMR Sedov of
-// levels 7-10, 32 layers on its complete level 7 made the FP32-bulk coarse
-// step slower, 0.771 -> 0.825 ms, and the FP64 one 1.4 % faster, so every
-// level keeps the coarse-fine tile.)
+// levels 7-10 with the levels stepped at once, 16 layers on its complete
+// level 7 instead of 8 left both precisions' coarse step within 1 %, and 32
+// layers made the FP32-bulk one 3 % slower and the FP64 one 1.3 % faster,
+// so every level keeps the coarse-fine tile.)
 TileCfg level_cfg(int l) {
   Context& c = ctx();
   (void)l;

@@ -1,8 +1,9 @@
 // rh_upload.cu — restriction of a fine level into its parent cells
 // (hydro/upload.f90:74-271 upload_fine; the reference's GPU path is
 // gpu_upload / upload_kernel, gpu/gpu_runner.cuf:1754-1784,
-// gpu/gpu_hydro.cuf:6972-7066).  One thread per fine oct reads the oct's
-// 8 x 5 record and writes the averages into the parent cell.
+// gpu/gpu_hydro.cuf:6972-7066).  The averages of a fine oct's 8 cells go
+// into its parent cell: one thread per (oct, variable) for the conservative
+// averages, one per oct when the internal energy is averaged instead.
 //
 // upload_fine first zeroes every refined cell of the coarse level; in a
 // single-rank mesh every refined cell has its child oct, so the averages
@@ -125,6 +126,43 @@ __global__ void upload_kernel(double* __restrict__ ud, float* __restrict__ uf, i
   }
 }
 
+// Conservative averages (interpol_var = 0): one thread per (fine oct,
+// variable), so that consecutive threads read consecutive runs of the oct
+// records (64 bytes each in FP64, 32 bytes of floats or the 64-byte energy
+// run in FP32-bulk) and a warp's loads coalesce; the per-oct thread above
+// strides 320 bytes from lane to lane.  Same sums in the same order.
+__global__ void upload_cons_kernel(double* __restrict__ ud, float* __restrict__ uf, int fp32,
+                                   const int2* __restrict__ father, long long o0, long long n) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n * 5) return;
+  const long long o = o0 + i / 5;
+  const int v = (int)(i - (i / 5) * 5);
+  const int2 fa = father[o];
+  if (fa.x < 0) return;
+  double u[8];
+  if (!fp32 || v == 4) {
+    const double2* s = reinterpret_cast<const double2*>(fp32 ? ud + o * kBulkD : ud + o * 40 + v * 8);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double2 q = s[k];
+      u[2 * k] = q.x;
+      u[2 * k + 1] = q.y;
+    }
+  } else {
+    const float4* s = reinterpret_cast<const float4*>(uf + o * kBulkF + v * 8);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const float4 q = s[k];
+      u[4 * k] = q.x; u[4 * k + 1] = q.y; u[4 * k + 2] = q.z; u[4 * k + 3] = q.w;
+    }
+  }
+  const double a = avg8(u);
+  const long long p = fa.x;
+  if (!fp32) ud[p * 40 + 8 * v + fa.y] = a;
+  else if (v < 4) uf[p * kBulkF + 8 * v + fa.y] = (float)a;
+  else ud[p * kBulkD + fa.y] = a;
+}
+
 }  // namespace
 }  // namespace rh
 
@@ -152,11 +190,17 @@ extern "C" int rh_upload(int head_idx, int num_octs, int internal_energy, double
     int rc = build_fathers();
     if (rc) return rc;
   }
-  const int threads = 128;
   const long long n = num_octs;
-  upload_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, c.stream>>>(
-      c.ud[c.cur], c.uf[c.cur], c.precision == RH_PREC_FP32_BULK ? 1 : 0, c.d_father, head_idx - 1, n,
-      internal_energy ? 1 : 0, smallr);
+  const int fp32 = c.precision == RH_PREC_FP32_BULK ? 1 : 0;
+  if (internal_energy) {
+    const int threads = 128;
+    upload_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, c.stream>>>(
+        c.ud[c.cur], c.uf[c.cur], fp32, c.d_father, head_idx - 1, n, 1, smallr);
+  } else {
+    const int threads = 160;  // 32 octs x 5 variables
+    upload_cons_kernel<<<(unsigned)((n * 5 + threads - 1) / threads), threads, 0, c.stream>>>(
+        c.ud[c.cur], c.uf[c.cur], fp32, c.d_father, head_idx - 1, n);
+  }
   RH_CUDA(cudaGetLastError());
   return RH_OK;
 }
