@@ -75,6 +75,18 @@ def profile_traffic(prec):
     return None if e is None else e.get("bytes_per_launch_256")
 
 
+def profile_pipes(prec):
+    """Pipe and issue fractions of the dominant kernel from the committed ncu
+    summary (an ncu capture, not measured by this run)."""
+    p = os.path.join(ROOT, "profiles", "godunov_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    e = d.get(prec)
+    return None if e is None else e.get("pipes")
+
+
 class ClockSampler:
     """SM clock and throttle reasons sampled (read-only NVML queries, every
     ~5 ms) while the timed region runs; falls back to nvidia-smi polling."""
@@ -827,6 +839,7 @@ def run_ours(args):
                  "ms_per_step": results["fp64"]["ms_per_step"],
                  "kernel_ms": kernel_ms["fp64"],
                  "roofline_frac": ncell * B_ALG["fp64"] / (kernel_ms["fp64"] * 1e-3) / 1e9 / peak,
+                 "pipes_ncu": profile_pipes("fp64"),
                  "clocks": results["fp64"]["clocks"]},
         "fp32_bulk_over_fp64": results["fp64"]["ms_per_step"] / ms,
         "step_latency_ms": {"p50": float(np.percentile(results[prec]["per_step"], 50)),
@@ -841,7 +854,7 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": profile_traffic(prec), "peak_kind": peak_kind,
                      "kernel": "godunov_pencil2_kernel (FP32-bulk)", "kernel_ms": kms,
-                     "bytes_per_cell_update": B_ALG[prec]},
+                     "bytes_per_cell_update": B_ALG[prec], "pipes_ncu": profile_pipes(prec)},
         "cpu_baseline": cpu,
         "accuracy": acc,
         "solve_latency_s": None if serve is None else {
