@@ -409,6 +409,7 @@ int rh_finalize(void) {
   cudaEventDestroy(c.ev1);
   for (cudaEvent_t e : c.ev_prolong) cudaEventDestroy(e);
   for (cudaEvent_t e : c.ev_level) cudaEventDestroy(e);
+  for (cudaEvent_t e : c.ev_gather) cudaEventDestroy(e);
   cudaEventDestroy(c.ev_side_start);
   cudaStreamDestroy(c.side);
   for (auto s : c.lev_stream) cudaStreamDestroy(s);
@@ -1490,16 +1491,17 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
       }
       RH_CUDA(cudaMalloc(&c.d_gcfl, sizeof(double) * 5 * (size_t)std::max(1LL, nblk)));
     }
-    if (c.ev_level.size() < (size_t)(c.levelmax + 1)) {
-      for (size_t k = c.ev_level.size(); k < (size_t)(c.levelmax + 1); ++k) {
+    for (auto* evs : {&c.ev_level, &c.ev_gather}) {
+      for (size_t k = evs->size(); k < (size_t)(c.levelmax + 1); ++k) {
         cudaEvent_t e;
         RH_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        c.ev_level.push_back(e);
+        evs->push_back(e);
       }
     }
     RH_CUDA(cudaEventRecord(c.ev_side_start, c.stream));
     for (auto s : c.lev_stream) RH_CUDA(cudaStreamWaitEvent(s, c.ev_side_start, 0));
-    std::vector<char> fused(c.levelmax + 1, 0), corrected(c.levelmax + 1, 0);
+    std::vector<char> fused(c.levelmax + 1, 0), corrected(c.levelmax + 1, 0), gathered(c.levelmax + 3, 0);
+    std::vector<cudaStream_t> lst(c.levelmax + 1, c.stream);  // each level's stream
     int j = 0;
     for (size_t i = lev.size(); i-- > 0; ++j) {
       const int l = lev[i];
@@ -1509,6 +1511,7 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
       fused[l] = key[0] == dx && key[1] == p->gamma && key[2] == p->smallr && key[5] == c.gravity[0] &&
                  key[6] == c.gravity[1] && key[7] == c.gravity[2] && key[3] == p->smallc;
       cudaStream_t st = j == 0 ? c.stream : c.lev_stream[(j - 1) % 3];
+      lst[l] = st;
       // a level whose father cells the gathers correct leaves them to the
       // gathers' CFL and has its partials reduced together with theirs
       const bool merge = fused[l] && corrected[l] && c.d_cflskip;
@@ -1518,8 +1521,10 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
       if (rc) return rc;
       RH_CUDA(cudaEventRecord(c.ev_level[l], st));
     }
-    for (int l : lev) RH_CUDA(cudaStreamWaitEvent(c.stream, c.ev_level[l], 0));
-    // the coarse-fine corrections, level by level into the coarser level's unew
+    // The coarse-fine corrections of each level with ghost octs, into the
+    // coarser level's unew: on the coarser level's stream (after its own
+    // pencils) once the level's pencils have filled the slots, so that a
+    // gather whose two levels are done runs while larger levels still step.
     long long goff = 0;
     for (int l : lev) {
       const LevelTables& T = c.levels[l];
@@ -1527,6 +1532,8 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
       const double* slots = c.d_gface_all + (size_t)(T.gbase - c.ngridmax) * 120;
       const int2* fathers = c.d_gfather + (T.gbase - c.ngridmax);
       const int lf = l - 1;  // the fathers' level
+      const cudaStream_t gs = lst[lf];
+      RH_CUDA(cudaStreamWaitEvent(gs, c.ev_level[l], 0));
       if (lf >= c.levelmin && fused[lf] && corrected[lf] && c.d_cflskip) {
         // the father level's CFL constants, as launch_level formed them
         const double dxf = dxl(lf);
@@ -1538,26 +1545,28 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
         const long long nb = (T.nghost + kGatherGhosts - 1) / kGatherGhosts;
         double* part = c.d_gcfl + 5 * goff;
         if (c.precision == RH_PREC_FP64)
-          coarse_gather_cfl_kernel<<<(unsigned)nb, kGatherThreads, 0, c.stream>>>(
+          coarse_gather_cfl_kernel<<<(unsigned)nb, kGatherThreads, 0, gs>>>(
               slots, T.nghost, fathers, c.d_refmask, c.ud[1 - c.cur], C, vol, part);
         else
-          coarse_gather_cfl_f32_kernel<<<(unsigned)nb, kGatherThreads, 0, c.stream>>>(
+          coarse_gather_cfl_f32_kernel<<<(unsigned)nb, kGatherThreads, 0, gs>>>(
               slots, T.nghost, fathers, c.d_refmask, c.uf[1 - c.cur], c.ud[1 - c.cur], C, vol, part);
         RH_CUDA(cudaGetLastError());
         const LevelTables& F = c.levels[lf];
-        reduce_partials_pair_kernel<<<1, 1024, 0, c.stream>>>(F.d_cfl_partial, F.npencil, part, nb,
-                                                              C.cdx_smallc, c.d_cfl + 5 * lf);
+        reduce_partials_pair_kernel<<<1, 1024, 0, gs>>>(F.d_cfl_partial, F.npencil, part, nb, C.cdx_smallc,
+                                                        c.d_cfl + 5 * lf);
         RH_CUDA(cudaGetLastError());
         goff += nb;
       } else {
         const unsigned nb = (unsigned)((T.nghost * 5ll + 255) / 256);
         if (c.precision == RH_PREC_FP64)
-          coarse_gather_kernel<<<nb, 256, 0, c.stream>>>(slots, T.nghost, fathers, c.ud[1 - c.cur]);
+          coarse_gather_kernel<<<nb, 256, 0, gs>>>(slots, T.nghost, fathers, c.ud[1 - c.cur]);
         else
-          coarse_gather_f32_kernel<<<nb, 256, 0, c.stream>>>(slots, T.nghost, fathers, c.uf[1 - c.cur],
-                                                             c.ud[1 - c.cur]);
+          coarse_gather_f32_kernel<<<nb, 256, 0, gs>>>(slots, T.nghost, fathers, c.uf[1 - c.cur],
+                                                       c.ud[1 - c.cur]);
         RH_CUDA(cudaGetLastError());
       }
+      RH_CUDA(cudaEventRecord(c.ev_gather[l], gs));
+      gathered[l] = 1;
     }
     c.cur = 1 - c.cur;
     for (int l : lev) {
@@ -1569,13 +1578,25 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
       c.cfl_on_uold[l] = fused[l];
       c.cfl_on_unew[l] = 0;
     }
+    // The restrictions, finest first, on the library stream (the finest
+    // level's): l+1 -> l writes level l's refined cells, which level l's
+    // pencils write too, and reads level l+1's cells once they are final
+    // (its own step, the gather of level l+2's corrections into it and the
+    // restriction l+2 -> l+1 before this one).
     for (size_t i = lev.size() - 1; i-- > 0;) {
       const int l = lev[i];
       if (l + 1 <= c.levelmax && c.noct[l + 1] > 0) {
-        rc = rh_upload(c.head[l + 1], c.noct[l + 1], p->interpol_var == 1 ? 1 : 0, p->gamma, p->smallr,
-                       p->smallc * p->smallc);
+        RH_CUDA(cudaStreamWaitEvent(c.stream, c.ev_level[l], 0));
+        RH_CUDA(cudaStreamWaitEvent(c.stream, c.ev_level[l + 1], 0));
+        if (gathered[l + 2]) RH_CUDA(cudaStreamWaitEvent(c.stream, c.ev_gather[l + 2], 0));
+        rc = upload_on(c.head[l + 1], c.noct[l + 1], p->interpol_var == 1 ? 1 : 0, p->smallr, c.stream);
         if (rc) return rc;
       }
+    }
+    // the whole step ordered before the library stream's next work
+    for (int l : lev) {
+      RH_CUDA(cudaStreamWaitEvent(c.stream, c.ev_level[l], 0));
+      if (gathered[l]) RH_CUDA(cudaStreamWaitEvent(c.stream, c.ev_gather[l], 0));
     }
     *dt = step_dt;
     if (c.state_check) return check_all_levels();

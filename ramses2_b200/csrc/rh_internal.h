@@ -117,6 +117,7 @@ struct Context {
   // rh_coarse_step's levels run concurrently on the library stream and these
   cudaStream_t lev_stream[3] = {nullptr, nullptr, nullptr};
   std::vector<cudaEvent_t> ev_level;
+  std::vector<cudaEvent_t> ev_gather;  // per level: its ghosts' gather into the coarser level done
   double* d_gface_all = nullptr;  // [ghost octs of the mesh][24][5], zeroed once per mesh
   uint8_t* d_cflskip = nullptr;   // [ngridmax, rounded up to 4] father cells of ghost octs (bit per cell)
   double* d_gcfl = nullptr;       // [gather blocks of all levels][5] CFL partials of the corrected cells
@@ -159,6 +160,8 @@ struct LevelSlots {
   const uint8_t* cflskip;  // cells the fused CFL epilogue leaves out (null: none)
   bool defer_reduce;       // no partial reduction: the caller merges it with the gather's
 };
+// rh_upload.cu: rh_upload's restriction of a level into its parents, on stream st
+int upload_on(int head_idx, int num_octs, int internal_energy, double smallr, cudaStream_t st);
 // rh_api.cu: one Godunov step of level l (all pencils, or `range`'s), and the
 // FP64 staging buffer of FP32-bulk transfers (grown on demand, kept).
 int launch_level(int l, double gamma, double smallr, double smallc, double dt, double dx, double smax_cap,

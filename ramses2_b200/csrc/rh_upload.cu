@@ -166,17 +166,12 @@ __global__ void upload_cons_kernel(double* __restrict__ ud, float* __restrict__ 
 }  // namespace
 }  // namespace rh
 
-using namespace rh;
+namespace rh {
 
-extern "C" int rh_upload(int head_idx, int num_octs, int internal_energy, double gamma, double smallr,
-                         double smallc2) {
+// rh_upload's work on a given stream (rh_coarse_step queues the restrictions
+// of its concurrent levels behind the work each one depends on).
+int upload_on(int head_idx, int num_octs, int internal_energy, double smallr, cudaStream_t st) {
   Context& c = ctx();
-  if (!c.inited || !c.have_mesh) {
-    set_error("rh_upload: rh_init and rh_set_mesh first");
-    return RH_ESTATE;
-  }
-  (void)gamma;
-  (void)smallc2;
   if (num_octs == 0) return RH_OK;
   if (head_idx < 1 || num_octs < 0 || head_idx - 1 + (long long)num_octs > c.ngridmax) {
     set_error("rh_upload: range outside the mesh");
@@ -194,13 +189,29 @@ extern "C" int rh_upload(int head_idx, int num_octs, int internal_energy, double
   const int fp32 = c.precision == RH_PREC_FP32_BULK ? 1 : 0;
   if (internal_energy) {
     const int threads = 128;
-    upload_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, c.stream>>>(
+    upload_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, st>>>(
         c.ud[c.cur], c.uf[c.cur], fp32, c.d_father, head_idx - 1, n, 1, smallr);
   } else {
     const int threads = 160;  // 32 octs x 5 variables
-    upload_cons_kernel<<<(unsigned)((n * 5 + threads - 1) / threads), threads, 0, c.stream>>>(
+    upload_cons_kernel<<<(unsigned)((n * 5 + threads - 1) / threads), threads, 0, st>>>(
         c.ud[c.cur], c.uf[c.cur], fp32, c.d_father, head_idx - 1, n);
   }
   RH_CUDA(cudaGetLastError());
   return RH_OK;
+}
+
+}  // namespace rh
+
+using namespace rh;
+
+extern "C" int rh_upload(int head_idx, int num_octs, int internal_energy, double gamma, double smallr,
+                         double smallc2) {
+  Context& c = ctx();
+  if (!c.inited || !c.have_mesh) {
+    set_error("rh_upload: rh_init and rh_set_mesh first");
+    return RH_ESTATE;
+  }
+  (void)gamma;
+  (void)smallc2;
+  return upload_on(head_idx, num_octs, internal_energy, smallr, c.stream);
 }
