@@ -21,8 +21,9 @@ extern "C" {
 int rh_set_tile(int txo, int tyo, int minb, int lz);
 /* Tile of the coarse-fine (multi-level) kernels; before rh_set_mesh, since a
  * mesh's interpolated ghost octs follow its pencils.  Default (the fastest on
- * the AMR Sedov of levels 7-10): 7x7 octs, 2 CTAs/SM, 8 layers for FP32-bulk; 8x4,
- * 2 CTAs/SM, 8 layers for FP64. */
+ * the AMR Sedov of levels 7-10): 7x7 octs, 2 CTAs/SM, 32 layers for FP32-bulk;
+ * 8x4, 2 CTAs/SM, 32 layers for FP64.  rh_set_mesh gives a partial level
+ * fewer layers (halved, down to 2) until its pencils fill two waves of CTAs. */
 int rh_set_amr_tile(int txo, int tyo, int minb, int lz);
 int rh_get_tile(int* txo, int* tyo, int* minb, int* lz);
 /* Compiled tile shapes of a precision mode; returns their count. */

@@ -502,7 +502,7 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
   if (rc) return rc;
   Context& c = ctx();
   // coarse-fine tile unless chosen: the fastest on the AMR Sedov of levels 7-10 per precision
-  if (!c.amr_cfg_set) c.amr_cfg = c.precision == RH_PREC_FP32_BULK ? TileCfg{7, 7, 2, 8} : TileCfg{8, 4, 2, 8};
+  if (!c.amr_cfg_set) c.amr_cfg = c.precision == RH_PREC_FP32_BULK ? TileCfg{7, 7, 2, 32} : TileCfg{8, 4, 2, 32};
   if (!m || !uold || !m->grid || !m->head || !m->noct) {
     set_error("rh_set_mesh: null pointer");
     return RH_EINVAL;
@@ -901,12 +901,11 @@ __global__ void coarse_gather_kernel(const double* __restrict__ gface, int nghos
 
 // Tile of level l's launches: the uniform tile on a single-level mesh, the
 // coarse-fine tile (kernels that handle refined cells and interpolated ghosts)
-// on every level of a multi-level mesh.  (A level that fills its box could
-// take deeper pencils, with fewer halo layers per cell; on the AMR Sedov of
-// levels 7-10 with the levels stepped at once, 16 layers on its complete
-// level 7 instead of 8 left both precisions' coarse step within 1 %, and 32
-// layers made the FP32-bulk one 3 % slower and the FP64 one 1.3 % faster,
-// so every level keeps the coarse-fine tile.)
+// on every level of a multi-level mesh.  A partial level takes the tile's
+// layers cut down by rh_set_mesh until it fills two waves of CTAs; a
+// complete level takes them all (on the AMR Sedov of levels 7-10, whose
+// level 7 is complete, 32 layers there instead of 8 made the coarse step
+// 4 % (FP32-bulk) and 1.4 % (FP64) faster, 64 layers 30 % / 20 % slower).
 TileCfg level_cfg(int l) {
   Context& c = ctx();
   (void)l;

@@ -55,7 +55,7 @@ struct LevelTables {
 
 struct Context {
   bool inited = false;
-  TileCfg amr_cfg{8, 4, 2, 8};  // tiles of multi-level meshes (coarse-fine kernels)
+  TileCfg amr_cfg{8, 4, 2, 32};  // tiles of multi-level meshes (coarse-fine kernels)
   bool amr_cfg_set = false;     // amr_cfg chosen by rh_set_amr_tile (else by precision at rh_set_mesh)
   int table_builder = 1;        // coarse-fine tables: 1 on the device, 0 on the host
   int state_check = 0;          // rh_coarse_step checks every level after set_uold (rh_set_state_check)
