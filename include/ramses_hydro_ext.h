@@ -23,7 +23,7 @@ int rh_set_tile(int txo, int tyo, int minb, int lz);
  * mesh's interpolated ghost octs follow its pencils.  Default (the fastest on
  * the AMR Sedov of levels 7-10): 7x7 octs, 2 CTAs/SM, 32 layers for FP32-bulk;
  * 8x4, 2 CTAs/SM, 32 layers for FP64.  rh_set_mesh gives a partial level
- * fewer layers (halved, down to 2) until its pencils fill two waves of CTAs. */
+ * fewer layers (halved, down to 2) until its pencils fill a wave of CTAs. */
 int rh_set_amr_tile(int txo, int tyo, int minb, int lz);
 int rh_get_tile(int* txo, int* tyo, int* minb, int* lz);
 /* Compiled tile shapes of a precision mode; returns their count. */

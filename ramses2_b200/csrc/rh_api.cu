@@ -567,13 +567,15 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
                           ((long long)c.box_nx[2] << (l - 1));
     if ((long long)c.noct[l] == box) continue;
     const long long gbase = (long long)c.ngridmax + nghost;
-    // A small level gets shorter pencils so that it still fills two waves of
+    // A small level gets shorter pencils so that it still fills a wave of
     // CTAs (its pencils are few; each one marches lz layers one after the
     // other): halve lz, down to 2, while the level's octs make fewer pencils
-    // than that.
+    // than that.  (One wave rather than two: rh_coarse_step runs the levels
+    // at once, and on the AMR Sedov of levels 7-10 that gave its level 10
+    // 16 layers instead of 8, 1.9 % (FP64) / 0.5 % (FP32-bulk) faster.)
     TileCfg lcfg = c.amr_cfg;
-    const long long waves2 = 2LL * c.sm_count * std::max(1, lcfg.minb);
-    while (lcfg.lz > 2 && (long long)c.noct[l] / ((long long)lcfg.txo * lcfg.tyo * lcfg.lz) < waves2) lcfg.lz /= 2;
+    const long long wave = (long long)c.sm_count * std::max(1, lcfg.minb);
+    while (lcfg.lz > 2 && (long long)c.noct[l] / ((long long)lcfg.txo * lcfg.tyo * lcfg.lz) < wave) lcfg.lz /= 2;
     if (c.table_builder) {
       cudaError_t e = cudaSuccess;
       if (!d_grid) {
@@ -902,7 +904,7 @@ __global__ void coarse_gather_kernel(const double* __restrict__ gface, int nghos
 // Tile of level l's launches: the uniform tile on a single-level mesh, the
 // coarse-fine tile (kernels that handle refined cells and interpolated ghosts)
 // on every level of a multi-level mesh.  A partial level takes the tile's
-// layers cut down by rh_set_mesh until it fills two waves of CTAs; a
+// layers cut down by rh_set_mesh until it fills a wave of CTAs; a
 // complete level takes them all (on the AMR Sedov of levels 7-10, whose
 // level 7 is complete, 32 layers there instead of 8 made the coarse step
 // 4 % (FP32-bulk) and 1.4 % (FP64) faster, 64 layers 30 % / 20 % slower).
