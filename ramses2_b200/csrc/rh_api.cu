@@ -1503,11 +1503,14 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
     for (auto s : c.lev_stream) RH_CUDA(cudaStreamWaitEvent(s, c.ev_side_start, 0));
     std::vector<char> fused(c.levelmax + 1, 0), corrected(c.levelmax + 1, 0), gathered(c.levelmax + 3, 0);
     std::vector<cudaStream_t> lst(c.levelmax + 1, c.stream);  // each level's stream
-    int j = 0;
-    for (size_t i = lev.size(); i-- > 0; ++j) {
-      const int l = lev[i];
-      const double dx = dxl(l);
+    for (int l : lev)
       if (l > c.levelmin && c.levels[l].nghost > 0) corrected[l - 1] = 1;
+    // coarsest level first: it waits for no prolongation, and the complete
+    // coarse level's deep pencils are the longest kernel of the step
+    for (size_t i = 0; i < lev.size(); ++i) {
+      const int l = lev[i];
+      const int j = (int)(lev.size() - 1 - i);  // 0: the finest level, on the library stream
+      const double dx = dxl(l);
       const double* key = &c.cfl_keys[8 * l];
       fused[l] = key[0] == dx && key[1] == p->gamma && key[2] == p->smallr && key[5] == c.gravity[0] &&
                  key[6] == c.gravity[1] && key[7] == c.gravity[2] && key[3] == p->smallc;
