@@ -322,8 +322,8 @@ def test_amr_coarse_step_native(bc, itype, ivar, spare):
     """rh_coarse_step (the whole level loop in one library call) against the
     oracle's coarse steps, FP64, three steps: same dt, 1e-12 per variable.
     With spare octs beyond the levels (ngridmax larger than the mesh) it
-    takes the level-by-level set_unew / set_uold path instead of the
-    whole-state copy and buffer swap."""
+    takes the level-by-level set_unew / set_uold path instead of the levels
+    stepped at once and the buffer swap."""
     m, P = amr_case(bc, itype, ivar)
     if spare:
         from ramses2_b200.mesh import Mesh
