@@ -391,6 +391,8 @@ int rh_init(int device_ordinal) {
   RH_CUDA(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
   for (auto& s : c.lev_stream) RH_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   RH_CUDA(cudaEventCreateWithFlags(&c.ev_side_start, cudaEventDisableTiming));
+  RH_CUDA(cudaStreamCreateWithFlags(&c.cfl_copy, cudaStreamNonBlocking));
+  RH_CUDA(cudaEventCreateWithFlags(&c.ev_cfl_copied, cudaEventDisableTiming));
   c.inited = true;
   return RH_OK;
 }
@@ -412,6 +414,9 @@ int rh_finalize(void) {
   for (cudaEvent_t e : c.ev_gather) cudaEventDestroy(e);
   cudaEventDestroy(c.ev_side_start);
   cudaStreamDestroy(c.side);
+  cudaEventDestroy(c.ev_cfl_copied);
+  cudaStreamDestroy(c.cfl_copy);
+  cudaFreeHost(c.h_cfl_next);
   for (auto s : c.lev_stream) cudaStreamDestroy(s);
   cudaStreamDestroy(c.stream);
   c = Context();
@@ -610,6 +615,10 @@ int rh_set_mesh(const rh_mesh_desc* m, const double* uold, int nvar, int twotond
     }
   }
   RH_CUDA(cudaMalloc(&c.d_cfl, sizeof(double) * 5 * (c.levelmax + 1)));
+  c.cfl_gen++;
+  cudaFreeHost(c.h_cfl_next);
+  c.h_cfl_next = nullptr;
+  RH_CUDA(cudaMallocHost(&c.h_cfl_next, sizeof(double) * 5 * (c.levelmax + 1)));
   {
     std::vector<uint8_t> ref((size_t)n, 0);
     for (long long i = 0; i < nused; ++i) {
@@ -822,6 +831,7 @@ static int cmpdt_enqueue(int head_idx, int num_octs, double dx, double gamma, do
                                                            c.d_refmask);
     RH_CUDA(cudaGetLastError());
     double* d_out = c.d_cfl + 5 * (l >= 0 ? l : 0);
+    c.cfl_gen++;
     reduce_partials_kernel<<<1, 1024, 0, c.stream>>>(c.d_scratch, nblk, 1e300, d_out);
     RH_CUDA(cudaGetLastError());
     RH_CUDA(cudaMemcpyAsync(host_out, d_out, sizeof(double) * 5, cudaMemcpyDeviceToHost, c.stream));
@@ -1200,6 +1210,7 @@ int launch_level(int l, double gamma, double smallr, double smallc, double dt, d
   }
   if (fuse_cfl && !range && !(slots && slots->defer_reduce)) {
     reduce_partials_kernel<<<1, 1024, 0, st>>>(T.d_cfl_partial, T.npencil, A.cfl.cdx_smallc, c.d_cfl + 5 * l);
+    c.cfl_gen++;
     RH_CUDA(cudaGetLastError());
   }
   return RH_OK;
@@ -1402,19 +1413,26 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
                              c.gravity[0], c.gravity[1], c.gravity[2]};
       all_cached = all_cached && c.cfl_on_uold[l] && std::equal(key, key + 8, &c.cfl_keys[8 * l]);
     }
-    if (all_cached) {
-      const int l0 = lev.front(), nl = lev.back() - l0 + 1;
-      RH_CUDA(cudaMemcpyAsync(h + 5 * l0, c.d_cfl + 5 * l0, sizeof(double) * 5 * nl, cudaMemcpyDeviceToHost,
-                              c.stream));
+    const int l0 = lev.front(), nl = lev.back() - l0 + 1;
+    if (all_cached && c.cfl_next_gen == c.cfl_gen && c.cfl_next_l0 == l0 && c.cfl_next_l1 == lev.back()) {
+      // copied by the previous call as soon as they were final: no wait
+      // for the rest of that step (its restrictions)
+      RH_CUDA(cudaEventSynchronize(c.ev_cfl_copied));
+      std::copy(c.h_cfl_next + 5 * l0, c.h_cfl_next + 5 * (l0 + nl), h + 5 * l0);
     } else {
-      for (int l : lev) {
-        bool queued = false;
-        rc = cmpdt_enqueue(c.head[l], c.noct[l], dxl(l), p->gamma, p->smallr, p->smallc, p->courant_factor,
-                           c.gravity, h + 5 * l, &queued);
-        if (rc) return rc;
+      if (all_cached) {
+        RH_CUDA(cudaMemcpyAsync(h + 5 * l0, c.d_cfl + 5 * l0, sizeof(double) * 5 * nl, cudaMemcpyDeviceToHost,
+                                c.stream));
+      } else {
+        for (int l : lev) {
+          bool queued = false;
+          rc = cmpdt_enqueue(c.head[l], c.noct[l], dxl(l), p->gamma, p->smallr, p->smallc, p->courant_factor,
+                             c.gravity, h + 5 * l, &queued);
+          if (rc) return rc;
+        }
       }
+      RH_CUDA(cudaStreamSynchronize(c.stream));
     }
-    RH_CUDA(cudaStreamSynchronize(c.stream));
     step_dt = 1e300;
     for (int l : lev) {
       const double* v = h + 5 * l;
@@ -1558,6 +1576,7 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
         const LevelTables& F = c.levels[lf];
         reduce_partials_pair_kernel<<<1, 1024, 0, gs>>>(F.d_cfl_partial, F.npencil, part, nb, C.cdx_smallc,
                                                         c.d_cfl + 5 * lf);
+        c.cfl_gen++;
         RH_CUDA(cudaGetLastError());
         goff += nb;
       } else {
@@ -1581,6 +1600,24 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
       // level's own partials plus its corrected cells' from the gathers
       c.cfl_on_uold[l] = fused[l];
       c.cfl_on_unew[l] = 0;
+    }
+    // every level's courant_fine values of the new state are final once its
+    // pencils and its gather's reduction ran: copy them to the host now, so
+    // that the next call's dt need not wait for the restrictions
+    bool all_fused = true;
+    for (int l : lev) all_fused = all_fused && fused[l];
+    if (all_fused) {
+      for (int l : lev) {
+        RH_CUDA(cudaStreamWaitEvent(c.cfl_copy, c.ev_level[l], 0));
+        if (gathered[l + 1]) RH_CUDA(cudaStreamWaitEvent(c.cfl_copy, c.ev_gather[l + 1], 0));
+      }
+      const int l0 = lev.front(), nl = lev.back() - l0 + 1;
+      RH_CUDA(cudaMemcpyAsync(c.h_cfl_next + 5 * l0, c.d_cfl + 5 * l0, sizeof(double) * 5 * nl,
+                              cudaMemcpyDeviceToHost, c.cfl_copy));
+      RH_CUDA(cudaEventRecord(c.ev_cfl_copied, c.cfl_copy));
+      c.cfl_next_gen = c.cfl_gen;
+      c.cfl_next_l0 = l0;
+      c.cfl_next_l1 = lev.back();
     }
     // The restrictions, finest first, on the library stream (the finest
     // level's): l+1 -> l writes level l's refined cells, which level l's

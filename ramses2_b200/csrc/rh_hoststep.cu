@@ -327,6 +327,7 @@ int rh_coarse_step_host(const rh_hydro_params* p, const double* host_in, double*
   // the fused CFL values of the new state (fixed reduction order of the schedule's pencils)
   const double cdx_smallc = p->courant_factor * dx / p->smallc;
   reduce_partials_kernel<<<1, 1024, 0, c.stream>>>(S.d_partial, S.npencil, cdx_smallc, c.d_cfl + 5 * l);
+  c.cfl_gen++;
   RH_CUDA(cudaGetLastError());
   // downloads of the finished chunks: FP32-bulk records unpacked to FP64 on
   // their own stream, so the copy stream only copies

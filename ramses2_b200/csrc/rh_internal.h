@@ -96,6 +96,15 @@ struct Context {
   double* d_scratch = nullptr;    // standalone cmpdt partials
   double* h_cfl = nullptr;        // pinned: courant_fine values read back, 5 per level
   size_t h_cfl_elems = 0;
+  // Every kernel that writes d_cfl bumps cfl_gen.  rh_coarse_step copies the
+  // levels' values of the state it leaves to h_cfl_next on cfl_copy as soon
+  // as they are final (before its restrictions end); the next call reads them
+  // from there while cfl_next_gen still equals cfl_gen.
+  unsigned long long cfl_gen = 0, cfl_next_gen = ~0ull;
+  double* h_cfl_next = nullptr;   // pinned, 5 per level
+  int cfl_next_l0 = -1, cfl_next_l1 = -1;
+  cudaStream_t cfl_copy = nullptr;
+  cudaEvent_t ev_cfl_copied = nullptr;
   double* d_stage64 = nullptr;    // FP64 staging of FP32-bulk uploads / downloads
   size_t stage64_bytes = 0;
   size_t scratch_elems = 0;
