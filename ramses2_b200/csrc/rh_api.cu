@@ -393,6 +393,7 @@ int rh_init(int device_ordinal) {
   RH_CUDA(cudaEventCreateWithFlags(&c.ev_side_start, cudaEventDisableTiming));
   RH_CUDA(cudaStreamCreateWithFlags(&c.cfl_copy, cudaStreamNonBlocking));
   RH_CUDA(cudaEventCreateWithFlags(&c.ev_cfl_copied, cudaEventDisableTiming));
+  RH_CUDA(cudaEventCreateWithFlags(&c.ev_cfl_ready, cudaEventDisableTiming));
   c.inited = true;
   return RH_OK;
 }
@@ -415,6 +416,7 @@ int rh_finalize(void) {
   cudaEventDestroy(c.ev_side_start);
   cudaStreamDestroy(c.side);
   cudaEventDestroy(c.ev_cfl_copied);
+  cudaEventDestroy(c.ev_cfl_ready);
   cudaStreamDestroy(c.cfl_copy);
   cudaFreeHost(c.h_cfl_next);
   for (auto s : c.lev_stream) cudaStreamDestroy(s);
@@ -1407,13 +1409,13 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
     if ((rc = cfl_host(&h))) return rc;
     // every level's values left by the previous step for these parameters:
     // one copy of the levels' slots instead of one per level
-    bool all_cached = lev.size() > 1;
+    bool all_cached = !lev.empty();
     for (int l : lev) {
       const double key[8] = {dxl(l), p->gamma, p->smallr, p->smallc, p->courant_factor,
                              c.gravity[0], c.gravity[1], c.gravity[2]};
       all_cached = all_cached && c.cfl_on_uold[l] && std::equal(key, key + 8, &c.cfl_keys[8 * l]);
     }
-    const int l0 = lev.front(), nl = lev.back() - l0 + 1;
+    const int l0 = lev.empty() ? 0 : lev.front(), nl = lev.empty() ? 0 : lev.back() - l0 + 1;
     if (all_cached && c.cfl_next_gen == c.cfl_gen && c.cfl_next_l0 == l0 && c.cfl_next_l1 == lev.back()) {
       // copied by the previous call as soon as they were final: no wait
       // for the rest of that step (its restrictions)
@@ -1658,6 +1660,21 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
                      p->smallc * p->smallc);
       if (rc) return rc;
     }
+  }
+  // every level's courant_fine values of the new state fused into its step:
+  // on their way to the host before the next call asks for them
+  bool all_fused = !lev.empty();
+  for (int l : lev) all_fused = all_fused && c.cfl_on_uold[l];
+  if (all_fused) {
+    const int l0 = lev.front(), nl = lev.back() - l0 + 1;
+    RH_CUDA(cudaEventRecord(c.ev_cfl_ready, c.stream));
+    RH_CUDA(cudaStreamWaitEvent(c.cfl_copy, c.ev_cfl_ready, 0));
+    RH_CUDA(cudaMemcpyAsync(c.h_cfl_next + 5 * l0, c.d_cfl + 5 * l0, sizeof(double) * 5 * nl,
+                            cudaMemcpyDeviceToHost, c.cfl_copy));
+    RH_CUDA(cudaEventRecord(c.ev_cfl_copied, c.cfl_copy));
+    c.cfl_next_gen = c.cfl_gen;
+    c.cfl_next_l0 = l0;
+    c.cfl_next_l1 = lev.back();
   }
   *dt = step_dt;
   if (c.state_check) return check_all_levels();  // the reference's gpu_debug scan after set_uold

@@ -104,7 +104,7 @@ struct Context {
   double* h_cfl_next = nullptr;   // pinned, 5 per level
   int cfl_next_l0 = -1, cfl_next_l1 = -1;
   cudaStream_t cfl_copy = nullptr;
-  cudaEvent_t ev_cfl_copied = nullptr;
+  cudaEvent_t ev_cfl_copied = nullptr, ev_cfl_ready = nullptr;
   double* d_stage64 = nullptr;    // FP64 staging of FP32-bulk uploads / downloads
   size_t stage64_bytes = 0;
   size_t scratch_elems = 0;

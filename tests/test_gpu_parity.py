@@ -458,6 +458,36 @@ def test_amr_coarse_step_courant_values_match_a_fresh_courant_fine(prec):
         gpu.close()
 
 
+@pytest.mark.parametrize("mesh_kind", ["amr", "uniform"])
+def test_coarse_step_dt_after_leaf_calls_in_between(mesh_kind):
+    """rh_coarse_step takes its dt from the courant_fine values the previous
+    call left (copied to the host early).  Leaf calls between two coarse
+    steps (a whole step through courant_fine / set_unew / godunov_fine /
+    set_uold) write new values: the next coarse step must take the dt of the
+    state they left, the one courant_fine now reports."""
+    from ramses2_b200.mesh import sedov_amr_mesh
+
+    if mesh_kind == "amr":
+        m, g = sedov_amr_mesh(3, 5, radius=0.3)
+    else:
+        m = uniform_mesh(5, nsubgrid=1, bc="outflow")
+        g = blast_state(m, 11, 1.4)
+    P = HydroParams.make(gamma=g, courant_factor=0.8, slope_type=2, riemann="hllc", interpol_var=0,
+                         interpol_type=1)
+    lev = [l for l in range(m.levelmin, m.levelmax + 1) if m.noct[l]]
+    gpu = GodunovGPU(m, P, precision="fp64")
+    try:
+        for _ in range(2):
+            gpu.coarse_step()
+        before = min(min(m.dx(l) / P.smallc, gpu.courant_fine(l)[4]) for l in lev)
+        amr_coarse_step(gpu, m)
+        expect = min(min(m.dx(l) / P.smallc, gpu.courant_fine(l)[4]) for l in lev)
+        assert expect != before
+        assert gpu.coarse_step() == expect
+    finally:
+        gpu.close()
+
+
 def test_amr_coarse_step_native_given_dt_fp32_bulk():
     """rh_coarse_step with the oracle's dt passed in (no courant_fine):
     FP32-bulk density within 1e-5 of the oracle's coarse step."""
