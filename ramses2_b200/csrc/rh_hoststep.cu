@@ -14,12 +14,12 @@
 // queues, made the copies queue behind kernels (26.6 ms per 256^3 step
 // against 18.1).
 // The pencil kernel is the one rh_coarse_step runs (the level's tile shape),
-// launched group by group over the schedule's own pencil tables, 8 layers
-// deep.  A cell's update does not depend on where pencils start and end, so
-// the new state is bitwise that of rh_set_grid_device + rh_coarse_step +
-// rh_transfer_grid_host, and so is the next dt (a minimum); the conserved
-// totals of the fused CFL epilogue are summed over other pencils, so they
-// agree to rounding.
+// launched group by group over the schedule's own pencil tables, 2 (FP32-bulk)
+// or 8 (FP64) layers deep.  A cell's update does not depend on where pencils
+// start and end, so the new state is bitwise that of rh_set_grid_device +
+// rh_coarse_step + rh_transfer_grid_host, and so is the next dt (a minimum);
+// the conserved totals of the fused CFL epilogue are summed over other
+// pencils, so they agree to rounding.
 //
 // The step's dt must be known before the first pencil runs.  A host that
 // loops passes the dt_next of its previous call: min(dx/smallc, courant dt)
@@ -44,7 +44,7 @@ struct HostStepSched {
   // what the schedule was built for: level, kernel tile shape, precision
   int level = -1, txo = 0, tyo = 0, minb = 0, precision = -1;
   long long noct = 0;
-  // the schedule's own pencil tables: the level's tile shape, kLz layers deep
+  // the schedule's own pencil tables: the level's tile shape, sched_lz() layers deep
   LevelTables T;
   int npencil = 0;
   // chunks: [k*C, min((k+1)*C, noct)) octs; uploaded in the order up_order
@@ -67,7 +67,12 @@ namespace {
 // Pencils this deep: a pencil needs its neighbourhood and a chunk waits for
 // the pencils that write it, so shallow pencils start earlier and release
 // chunks sooner; the pencils' extra halo work is hidden behind the copies.
-constexpr int kLz = 8;
+// FP32-bulk takes 2 layers, FP64 8: on a 256^3 step 2 layers brought the
+// FP32-bulk step from 18.7 to 18.2 ms (the first chunks go back sooner, and
+// the extra halo work of its fast kernel stays hidden behind the copies) and
+// the FP64 one from 16.3 to 18.2 ms (its kernel, twice as slow, no longer
+// keeps pace).
+int sched_lz(int precision) { return precision == RH_PREC_FP32_BULK ? 2 : 8; }
 // 128 chunks of 16,384 octs (5.2 MB of FP64 state per copy) for a 256^3
 // level: on one box 18.8-18.9 ms per FP32-bulk step, against 18.3-19.6 with
 // 256 chunks and 20-21 with 64 (fewer chunks leave a longer tail of downloads
@@ -102,7 +107,7 @@ int build_sched(int l, HostStepSched& S) {
   const long long o0 = c.head[l] - 1;  // 0 for the single level of a mesh
   const TileCfg& main = c.cfg;
   TileCfg cfg = main;
-  cfg.lz = kLz;
+  cfg.lz = sched_lz(c.precision);
   S.level = l;
   S.txo = main.txo;
   S.tyo = main.tyo;
