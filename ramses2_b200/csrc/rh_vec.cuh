@@ -66,6 +66,15 @@ __device__ __forceinline__ float2 operator-(float2 a) { return make_float2(-a.x,
 __device__ __forceinline__ float2 operator-(float2 a, float2 b) { return __fadd2_rn(a, -b); }
 __device__ __forceinline__ float2 operator*(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a - b rounded once per lane, never merged into a multiply-add with the
+// products that formed a or b
+__device__ __forceinline__ float2 vsub_nc(float2 a, float2 b) {
+  float2 r;
+  asm("sub.rn.f32 %0, %2, %4;\n\tsub.rn.f32 %1, %3, %5;"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
 // Fortran MIN / MAX of ordered (NaN-free) operands as one FMNMX per lane;
 // the results differ from a compare-and-select at most in the sign of a zero.
 __device__ __forceinline__ float2 vmin(float2 a, float2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
