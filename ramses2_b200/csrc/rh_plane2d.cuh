@@ -105,7 +105,14 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
   Columns<G> col;
   col.init(t, ox0, oy0, A);
   const bool active = t < G::NRC;
-  V qmx[5], qmy[5];
+  // FP32-bulk 7x7 tiles (16-wide ring rows, each inside a warp): x faces by
+  // warp shuffle and both y faces solved by each cell, so the flux exchange
+  // needs no barrier of its own (as the pencil body); FS then holds the
+  // lower and upper y states
+  constexpr bool kOneBar = !F64 && G::RW == 16;
+  V qmx[5], qmy[5], qpx[5], dfx[5];
+#pragma unroll
+  for (int n = 0; n < 5; ++n) qpx[n] = V{};
   // (C) slopes, predictor and x/y interface states of the ring cells
   if (active) {
     V cur[5], xm[5], xp[5], ym[5], yp[5];
@@ -137,15 +144,39 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
     trace_cell(cur, irc, d, qm, qp, H);
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
-      FS[n * G::NRC + t] = qp[0][n];
-      FS[(5 + n) * G::NRC + t] = qp[1][n];
+      if (kOneBar) {
+        FS[n * G::NRC + t] = qp[1][n];
+        FS[(5 + n) * G::NRC + t] = qm[1][n];
+        qpx[n] = qp[0][n];
+      } else {
+        FS[n * G::NRC + t] = qp[0][n];
+        FS[(5 + n) * G::NRC + t] = qp[1][n];
+      }
       qmx[n] = qm[0][n];
       qmy[n] = qm[1][n];
     }
   }
+  if constexpr (kOneBar) {
+    V qr[5], fxr[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      qr[n].x = __shfl_down_sync(0xffffffffu, qpx[n].x, 1);
+      qr[n].y = __shfl_down_sync(0xffffffffu, qpx[n].y, 1);
+      fxr[n] = V{};
+    }
+    if (active && col.rx >= -1 && col.rx < G::CX && col.ry >= 0 && col.ry < G::CY)
+      riemann_dtdx<V, RIEMANN>(qmx, qr, fxr, H);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      V fl;
+      fl.x = __shfl_up_sync(0xffffffffu, fxr[n].x, 1);
+      fl.y = __shfl_up_sync(0xffffffffu, fxr[n].y, 1);
+      dfx[n] = vsub_nc(fl, fxr[n]);
+    }
+  }
   __syncthreads();
   // (D) x flux at the right face and y flux at the top face
-  if (active) {
+  if (!kOneBar && active) {
     if (col.rx >= -1 && col.rx < G::CX && col.ry >= 0 && col.ry < G::CY) {
       V qr[5], f[5];
 #pragma unroll
@@ -167,7 +198,7 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
       for (int n = 0; n < 5; ++n) FY[n * G::NRC + t] = fy[n];
     }
   }
-  __syncthreads();
+  if (!kOneBar) __syncthreads();
   // (E) conservative update of the tile's cells, written to both planes
   if constexpr (F64) {
     if (active && col.interior && col.in_domain_xy) {
@@ -204,17 +235,40 @@ __device__ __forceinline__ void plane2d_body(const LevelArgs& A, const StateArgs
       const float2* FY = FXY + 5 * G::NRC;
       const float* oa = S.uold_f + (size_t)octa * kBulkF + c;
       const float* ob = S.uold_f + (size_t)octb * kBulkF + c;
+      float2 dx_[5], dy_[5];
+      if constexpr (kOneBar) {
+        const int tn = t + G::RW, ts = t - G::RW;
+        const float2 qlt[5] = {qmy[0], qmy[2], qmy[1], qmy[3], qmy[4]};
+        const float2 qrt[5] = {FS[0 * G::NRC + tn], FS[2 * G::NRC + tn], FS[1 * G::NRC + tn], FS[3 * G::NRC + tn],
+                               FS[4 * G::NRC + tn]};
+        const float2 qlb[5] = {FS[5 * G::NRC + ts], FS[7 * G::NRC + ts], FS[6 * G::NRC + ts], FS[8 * G::NRC + ts],
+                               FS[9 * G::NRC + ts]};
+        const float2 qrb[5] = {FS[0 * G::NRC + t], FS[2 * G::NRC + t], FS[1 * G::NRC + t], FS[3 * G::NRC + t],
+                               FS[4 * G::NRC + t]};
+        float2 ft[5], fb[5];
+        riemann_dtdx<float2, RIEMANN>(qlt, qrt, ft, H);
+        riemann_dtdx<float2, RIEMANN>(qlb, qrb, fb, H);
+        const int un[5] = {0, 2, 1, 3, 4};
+#pragma unroll
+        for (int n = 0; n < 5; ++n) {
+          dx_[n] = dfx[n];
+          dy_[n] = vsub_nc(fb[un[n]], ft[un[n]]);
+        }
+      } else {
+#pragma unroll
+        for (int n = 0; n < 5; ++n) {
+          dx_[n] = FX[n * G::NRC + t - 1] - FX[n * G::NRC + t];
+          dy_[n] = FY[n * G::NRC + t - G::RW] - FY[n * G::NRC + t];
+        }
+      }
       float2 u2[4];
 #pragma unroll
       for (int n = 0; n < 4; ++n) {
         const float2 base = make_float2(oa[8 * n], ob[8 * n]);
-        u2[n] = (base + (FX[n * G::NRC + t - 1] - FX[n * G::NRC + t])) +
-                (FY[n * G::NRC + t - G::RW] - FY[n * G::NRC + t]);
+        u2[n] = (base + dx_[n]) + dy_[n];
       }
-      const double ea = (S.uold_d[(size_t)octa * kBulkD + c] + (double)(FX[4 * G::NRC + t - 1].x - FX[4 * G::NRC + t].x)) +
-                        (double)(FY[4 * G::NRC + t - G::RW].x - FY[4 * G::NRC + t].x);
-      const double eb = (S.uold_d[(size_t)octb * kBulkD + c] + (double)(FX[4 * G::NRC + t - 1].y - FX[4 * G::NRC + t].y)) +
-                        (double)(FY[4 * G::NRC + t - G::RW].y - FY[4 * G::NRC + t].y);
+      const double ea = (S.uold_d[(size_t)octa * kBulkD + c] + (double)dx_[4].x) + (double)dy_[4].x;
+      const double eb = (S.uold_d[(size_t)octb * kBulkD + c] + (double)dx_[4].y) + (double)dy_[4].y;
       // the z flux differences, exact +0
       float ua[4], ub[4];
 #pragma unroll
