@@ -134,10 +134,10 @@ int rh_timer_stop(float* ms);
 /* ---- for callers that cannot allocate -------------------------------------
  * rh_cmpdt_noalloc has no counterpart in the reference (RAMSES II's
  * gpu_cmpdt_2 borrows scratch from a device array it owns).  It serves hosts
- * that must not let a library call cudaMalloc/cudaFree: code capturing CUDA
- * graphs, solvers whose own memory manager hands out all device memory under
- * a fixed budget, and tight loops that cannot afford the device-wide
- * synchronisation an allocation implies.
+ * that must not let a library call cudaMalloc/cudaFree: solvers whose own
+ * memory manager hands out all device memory under a fixed budget, and tight
+ * loops that cannot afford the device-wide synchronisation an allocation
+ * implies.
  *
  * courant_fine over a caller-owned FP64 state, allocating nothing:
  * d_uold    device pointer to num_octs oct records in the reference layout

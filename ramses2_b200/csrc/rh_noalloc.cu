@@ -1,10 +1,9 @@
 // rh_noalloc.cu — a Courant/conservation reduction that allocates nothing.
 //
-// Some hosts cannot let a library call cudaMalloc: code that records CUDA
-// graphs while other work is being captured, solvers whose memory manager
-// owns every byte of device memory (a fixed HBM budget handed out to resident
-// problems), and time-critical loops that must not take the device-wide
-// synchronisation cudaMalloc/cudaFree imply.  rh_cmpdt_noalloc serves them:
+// Some hosts cannot let a library call cudaMalloc: solvers whose memory
+// manager owns every byte of device memory (a fixed HBM budget handed out to
+// resident problems), and time-critical loops that must not take the
+// device-wide synchronisation cudaMalloc/cudaFree imply.  rh_cmpdt_noalloc serves them:
 // the caller passes its own device input (the oct state) and device output
 // (5 doubles), and the per-block partial sums live in a file-scope device
 // array of fixed size instead of library-allocated memory.
