@@ -2,7 +2,8 @@
 
 Every ``csrc/*.cu`` is compiled to an object under ``_build/`` in parallel and
 linked into ``ramses2_b200/librh_b200.so``; the library is rebuilt only when a
-source or header is newer than it.
+source or header is newer than it or the set of sources changed since the
+last link (a deleted instantiation unit must not stay in the library).
 """
 import concurrent.futures as cf
 import glob
@@ -15,6 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "librh_b200.so")
+STAMP = os.path.join(BUILD, "sources.txt")  # the sources of the last link, one name per line
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include"),
@@ -35,7 +37,14 @@ def up_to_date():
     if not os.path.exists(LIB):
         return False
     t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(d) <= t for d in _deps())
+    if not all(os.path.getmtime(d) <= t for d in _deps()):
+        return False
+    try:
+        with open(STAMP) as f:
+            linked = f.read().split()
+    except OSError:
+        return True  # a library shipped without its build folder
+    return linked == [os.path.basename(s) for s in _sources()]
 
 
 def _compile(src, extra):
@@ -63,6 +72,8 @@ def build(force=False, verbose=False, jobs=None, ptxas_info=False):
     cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
+    with open(STAMP, "w") as f:
+        f.write("\n".join(os.path.basename(s) for s in _sources()) + "\n")
     return LIB
 
 
