@@ -421,11 +421,17 @@ template <typename T, class G, bool DENSE = false> struct Stager {
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
   }
-  __device__ __forceinline__ void issue(int row) {
+  // The table entry this thread's copy of layer row reads (-1 for threads
+  // that issue none): loaded ahead of issue(row, oct), the copy does not wait
+  // for the table read.
+  __device__ __forceinline__ int entry(int row) const {
+    return threadIdx.x < G::NSLOT ? oct_at(row, threadIdx.x) : -1;
+  }
+  __device__ __forceinline__ void issue(int row) { issue(row, entry(row)); }
+  __device__ __forceinline__ void issue(int row, int oct) {
     const int t = threadIdx.x;
     if (t < G::NSLOT) {
       const int st = (rb() + row) % G::NSTAGE;
-      const int oct = oct_at(row, t);
       fence_proxy_async_smem();
       if (oct >= 0) {
         mbar_arrive_expect_tx(&bar[st], Store<T>::kBytes);
