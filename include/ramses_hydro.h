@@ -69,7 +69,7 @@ typedef struct rh_hydro_params {
     double smallr;
     double smallc;
     double courant_factor;
-    double difmag;          /* must be 0: cmpdiff (umuscl.f90:2443) is not on this path */
+    double difmag;          /* > 0: cmpdivu/cmpdiff (umuscl.f90:2392-2540), rh_coarse_step on one FP64 level */
     int32_t slope_type;     /* 0 none, 1 minmod, 2 moncen, 3 multi-d positivity  */
     int32_t riemann;        /* RH_RIEMANN_*                                      */
     int32_t interpol_var;   /* 0: rho, rho u, E   1: rho, rho u, rho e           */

@@ -59,7 +59,11 @@ int rh_level_ghosts(int ilevel, int* gsrc_oct, unsigned char* gsrc_cf, int* gfat
  * changed.  There the step also leaves every level's courant_fine values of
  * the new state (the pencils' fused epilogue for the cells they finish, the
  * correcting gather for the father cells), so the next call's rh_cmpdt of
- * every level reads five numbers instead of the state. */
+ * every level reads five numbers instead of the state.
+ * p->difmag > 0 adds unsplit's artificial diffusion (cmpdivu / cmpdiff,
+ * hydro/umuscl.f90:2392-2540) to the step of a mesh of one complete level in
+ * FP64; other meshes and FP32-bulk return RH_EINVAL with difmag > 0.  The
+ * leaf call rh_godunov, like mtl_godunov, takes no difmag. */
 int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl);
 
 /* Coarse-fine update of the father cells (unew of level l-1 += or -= the

@@ -4,7 +4,8 @@
 // Godunov step for NDIM=3, hydro only (no MHD, no NENER, no passive scalars),
 // following the reference Fortran routine by routine:
 //   hydro/umuscl.f90        unsplit 20-292, trace3d 860-1466, cmpflxm 1472-1607,
-//                           ctoprim 1739-1901, uslope 1906-2387
+//                           ctoprim 1739-1901, uslope 1906-2387,
+//                           cmpdivu 2392-2440, cmpdiff 2444-2540 (difmag > 0)
 //   hydro/godunov_utils.f90 cmpdt 228-333, riemann_llf 338-481,
 //                           riemann_hll 486-633, riemann_hllc 638-852
 //   hydro/godunov_fine.f90  godunov_fine 43-79, godfine1 244-1342
@@ -28,7 +29,9 @@
 //  * Parent keys of negative fine keys use floor division; the reference's
 //    integer division truncates toward zero (nbors_utils.f90:190-196), which
 //    only matters for a missing fine oct on a non-periodic low face.
-//  * difmag>0 (cmpdivu/cmpdiff) is rejected, as in the CUDA path.
+//  * difmag > 0 (cmpdivu/cmpdiff) has no reference output to pin it to (the
+//    reference's GPU and Metal kernels have no artificial diffusion); it
+//    rests on this restatement of the two Fortran routines.
 
 #include "rh_oracle.h"
 
@@ -443,7 +446,72 @@ void cmpflxm(Work& W, int xdim, int ilo, int ihi, int jlo, int jhi, int klo, int
       }
 }
 
-// unsplit, umuscl.f90:20-292 (NDIM=3, hydro, difmag=0)
+// cmpdivu, umuscl.f90:2392-2440 (NDIM=3): velocity divergence at the cell
+// corners, div(i,j,k) at the corner shared by cells i-1..i, j-1..j, k-1..k.
+void cmpdivu(Work& W, double dx, std::vector<double>& div) {
+  Stencil& q = W.qloc;
+  const int e = W.if2 - W.if1 + 1;
+  div.assign((size_t)e * e * e, 0.0);
+  const double fact = (half * half) / dx;  // half**(ndim-1)/dx
+  for (int k = W.if1; k <= W.if2; ++k)
+    for (int j = W.if1; j <= W.if2; ++j)
+      for (int i = W.if1; i <= W.if2; ++i) {
+        double ux = zero, vy = zero, wz = zero;
+        ux = ux + fact * (q(i, j, k, 2) - q(i - 1, j, k, 2));
+        ux = ux + fact * (q(i, j - 1, k, 2) - q(i - 1, j - 1, k, 2));
+        vy = vy + fact * (q(i, j, k, 3) - q(i, j - 1, k, 3) + q(i - 1, j, k, 3) - q(i - 1, j - 1, k, 3));
+        ux = ux + fact * (q(i, j, k - 1, 2) - q(i - 1, j, k - 1, 2) + q(i, j - 1, k - 1, 2) -
+                          q(i - 1, j - 1, k - 1, 2));
+        vy = vy + fact * (q(i, j, k - 1, 3) - q(i, j - 1, k - 1, 3) + q(i - 1, j, k - 1, 3) -
+                          q(i - 1, j - 1, k - 1, 3));
+        wz = wz + fact * (q(i, j, k, 4) - q(i, j, k - 1, 4) + q(i, j - 1, k, 4) - q(i, j - 1, k - 1, 4) +
+                          q(i - 1, j, k, 4) - q(i - 1, j, k - 1, 4) + q(i - 1, j - 1, k, 4) -
+                          q(i - 1, j - 1, k - 1, 4));
+        div[(size_t)(i - W.if1) + (size_t)e * ((j - W.if1) + (size_t)e * (k - W.if1))] = ux + vy + wz;
+      }
+}
+
+// cmpdiff, umuscl.f90:2444-2540 (NDIM=3, hydro): adds to each face flux
+// dt * difmag * min(0, mean corner divergence of the face) times the jump of
+// the conserved variables across the face (W.flux holds F dt/dx).
+void cmpdiff(Work& W, const std::vector<double>& div, double dt, double difmag) {
+  Stencil& u = W.uloc;
+  const int e = W.if2 - W.if1 + 1;
+  auto D = [&](int i, int j, int k) {
+    return div[(size_t)(i - W.if1) + (size_t)e * ((j - W.if1) + (size_t)e * (k - W.if1))];
+  };
+  const double fact = half * half;  // half**(ndim-1)
+  const int kx2 = std::max(W.if1, W.iu2 - 2), ilo = W.iu1 + 2, ihi = W.iu2 - 2;
+  for (int n = 1; n <= 5; ++n) {
+    for (int k = W.if1; k <= kx2; ++k)
+      for (int j = W.if1; j <= kx2; ++j)
+        for (int i = W.if1; i <= W.if2; ++i) {
+          double div1 = fact * D(i, j, k);
+          div1 = div1 + fact * D(i, j + 1, k);
+          div1 = div1 + fact * (D(i, j, k + 1) + D(i, j + 1, k + 1));
+          div1 = difmag * fmin2(zero, div1);
+          W.flux(i, j, k, n, 1) = W.flux(i, j, k, n, 1) + dt * div1 * (u(i, j, k, n) - u(i - 1, j, k, n));
+        }
+    for (int k = W.if1; k <= kx2; ++k)
+      for (int j = W.if1; j <= W.if2; ++j)
+        for (int i = ilo; i <= ihi; ++i) {
+          double div1 = zero;
+          div1 = div1 + fact * (D(i, j, k) + D(i + 1, j, k));
+          div1 = div1 + fact * (D(i, j, k + 1) + D(i + 1, j, k + 1));
+          div1 = difmag * fmin2(zero, div1);
+          W.flux(i, j, k, n, 2) = W.flux(i, j, k, n, 2) + dt * div1 * (u(i, j, k, n) - u(i, j - 1, k, n));
+        }
+    for (int k = W.if1; k <= W.if2; ++k)
+      for (int j = ilo; j <= ihi; ++j)
+        for (int i = ilo; i <= ihi; ++i) {
+          double div1 = fact * (D(i, j, k) + D(i + 1, j, k) + D(i, j + 1, k) + D(i + 1, j + 1, k));
+          div1 = difmag * fmin2(zero, div1);
+          W.flux(i, j, k, n, 3) = W.flux(i, j, k, n, 3) + dt * div1 * (u(i, j, k, n) - u(i, j, k - 1, n));
+        }
+  }
+}
+
+// unsplit, umuscl.f90:20-292 (NDIM=3, hydro)
 void unsplit(Work& W, const double* g, double dx, double dt, const rh_hydro_params& P) {
   int ilo = std::min(1, W.iu1 + 2), ihi = std::max(1, W.iu2 - 2);
   double smax_cap = P.courant_factor * dx / dt;  // umuscl.f90:99
@@ -459,6 +527,11 @@ void unsplit(Work& W, const double* g, double dx, double dt, const rh_hydro_para
       for (int k = fk1; k <= fk2; ++k)
         for (int j = fj1; j <= fj2; ++j)
           for (int i = fi1; i <= fi2; ++i) W.flux(i, j, k, n, d) = W.fx(i, j, k, n) * dt / dx;
+  }
+  if (P.difmag > 0.0) {  // umuscl.f90:273-283
+    std::vector<double> div;
+    cmpdivu(W, dx, div);
+    cmpdiff(W, div, dt, P.difmag);
   }
 }
 
@@ -849,7 +922,6 @@ void godfine1(MeshCtx& C, GhostCache& G, Work& W, int ind_grid, int ilevel, doub
 
 bool check_params(const rh_hydro_params* p) {
   if (!p) { g_err = "null params"; return false; }
-  if (p->difmag > 0.0) { g_err = "difmag>0 (cmpdiff) is not supported"; return false; }
   if (p->slope_type < 0 || p->slope_type > 3) { g_err = "slope_type must be 0..3"; return false; }
   if (p->riemann < 1 || p->riemann > 3) { g_err = "riemann must be llf(1), hll(2) or hllc(3)"; return false; }
   return true;

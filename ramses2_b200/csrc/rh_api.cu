@@ -254,6 +254,7 @@ static void free_tables(LevelTables& t) {
 static void free_state() {
   Context& c = ctx();
   free_host_schedule();
+  free_diffusion();
   cudaFree(c.d_gface_all);
   c.d_gface_all = nullptr;
   cudaFree(c.d_cflskip);
@@ -1402,6 +1403,12 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
   for (int l = c.levelmin; l <= c.levelmax; ++l)
     if (c.noct[l] > 0) lev.push_back(l);
   auto dxl = [&](int l) { return c.boxlen / std::ldexp(1.0, l); };
+  // artificial diffusion (unsplit's cmpdivu/cmpdiff when difmag > 0)
+  const bool diffuse = p->difmag > 0.0;
+  if (diffuse && (lev.size() != 1 || !diffusion_supported(lev[0]))) {
+    set_error("rh_coarse_step: difmag > 0 (cmpdivu/cmpdiff) runs on a mesh of one complete level in FP64 only");
+    return RH_EINVAL;
+  }
   double step_dt = *dt;
   if (!(step_dt > 0)) {
     // courant_fine of every level queued back to back, one wait for all
@@ -1654,6 +1661,12 @@ int rh_coarse_step(const rh_hydro_params* p, double* dt, double* cfl) {
                     p->smallr, p->smallc * p->smallc, step_dt, dx, p->courant_factor * dx / step_dt, p->slope_type,
                     p->riemann, c.gravity);
     if (rc) return rc;
+    if (diffuse) {
+      // the diffusive face fluxes added to unew; the fused courant_fine
+      // values of the pencils no longer describe it
+      if ((rc = diffuse_level(l, step_dt, dx, p->difmag, p->smallr, c.gravity))) return rc;
+      c.cfl_on_unew[l] = 0;
+    }
     if ((rc = rh_set_uold(c.head[l], c.noct[l]))) return rc;
     if (i + 1 < lev.size() && l + 1 <= c.levelmax && c.noct[l + 1] > 0) {
       rc = rh_upload(c.head[l + 1], c.noct[l + 1], p->interpol_var == 1 ? 1 : 0, p->gamma, p->smallr,

@@ -236,8 +236,9 @@ int rh_coarse_step_host(const rh_hydro_params* p, const double* host_in, double*
   const double dx = l >= 0 ? c.boxlen / std::ldexp(1.0, l) : 0.0;
   const double g[3] = {c.gravity[0], c.gravity[1], c.gravity[2]};
   int rc;
-  if (nlev != 1 || c.noct[l] != c.ngridmax || c.nsubgrid != 1) {
-    // several levels (or spare octs): the same calls one after the other
+  if (nlev != 1 || c.noct[l] != c.ngridmax || c.nsubgrid != 1 || p->difmag > 0.0) {
+    // several levels (or spare octs), or artificial diffusion: the same
+    // calls one after the other
     if ((rc = rh_set_grid_device(host_in, c.ngridmax, 5, 8))) return rc;
     if ((rc = rh_coarse_step(p, dt, nullptr))) return rc;
     if ((rc = rh_transfer_grid_host(host_out, c.ngridmax, 5, 8))) return rc;

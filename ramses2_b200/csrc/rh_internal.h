@@ -130,6 +130,12 @@ struct Context {
   double* d_gface_all = nullptr;  // [ghost octs of the mesh][24][5], zeroed once per mesh
   uint8_t* d_cflskip = nullptr;   // [ngridmax, rounded up to 4] father cells of ghost octs (bit per cell)
   double* d_gcfl = nullptr;       // [gather blocks of all levels][5] CFL partials of the corrected cells
+  // artificial diffusion (rh_diffusion.cu): oct coordinates -> oct index of
+  // the level it was built for, and the corner divergences
+  int* d_difmap = nullptr;
+  int difmap_level = -1;
+  double* d_div = nullptr;
+  size_t div_elems = 0;
 };
 
 Context& ctx();
@@ -138,6 +144,13 @@ Context& ctx();
 int build_amr_tables(int l, const TileCfg& cfg, long long gbase);
 int upload_amr_tables(int l);
 int prolong_ghosts(int l, double smallr, cudaStream_t st = nullptr);  // null: the library stream
+
+// artificial diffusion, difmag > 0 (rh_diffusion.cu): adds cmpdiff's face
+// fluxes of level l to unew after its pencils; a mesh of one complete level
+// in FP64 only (diffusion_supported)
+bool diffusion_supported(int l);
+int diffuse_level(int l, double dt, double dx, double difmag, double smallr, const double* gravity);
+void free_diffusion();
 // coarse-fine levels built on the device (rh_amr_tables.cu): same tables as
 // build_amr_tables; *d_gfather_out receives the level's ghost fathers (device)
 int build_amr_tables_device(int l, const TileCfg& cfg, long long gbase, const rh_oct* d_grid, int2** d_gfather_out);
