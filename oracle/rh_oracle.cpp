@@ -17,9 +17,13 @@
 // Expression order follows the Fortran source left to right; build with
 // -ffp-contract=off so no FMA contraction changes the rounding.
 //
-// Parity status: unpinned against the reference binary (no Fortran compiler
-// in the image, no golden vectors in the reference for this path); pinned by
-// known-answer physics tests in tests/.
+// Parity status: the Fortran binary cannot be built (no Fortran compiler in
+// the image) and the reference holds no golden vectors for this path.  The
+// restatement is pinned to the reference's own code where it exists in a
+// buildable form: its Metal hydro, upload and flag shaders compiled as C++,
+// as written (FP32) and with their arithmetic in FP64
+// (tests/test_oracle_pin_ref.py), and its Python output reader
+// (tests/test_files_host.py); beyond those, by known-answer physics tests.
 //
 // Deliberate deviations (documented, none reachable in the configs):
 //  * Boundary ghost octs are built recursively from their reference oct
